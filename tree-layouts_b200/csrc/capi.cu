@@ -1,0 +1,236 @@
+// extern "C" surface of libtreelayouts.so (declared in include/tree_layouts.h),
+// plus the host-only pieces: mvEB position tables and status plumbing.
+#include <atomic>
+#include <cstdlib>
+#include <cstring>
+
+#include "geometry.cuh"
+#include "internal.h"
+
+namespace tl {
+
+static thread_local int t_last_cuda_error = 0;
+void record_cuda_error(cudaError_t e) { t_last_cuda_error = (int)e; }
+
+static std::atomic<unsigned int> g_spin_limit{1u << 22};  // ~1 s of 256 ns sleeps
+static std::atomic<int> g_force_timeout{0};
+unsigned int debug_spin_limit() { return g_spin_limit.load(); }
+bool debug_force_timeout() { return g_force_timeout.load() != 0; }
+void debug_set_wait(unsigned int spin_limit, int force_timeout) {
+    g_spin_limit.store(spin_limit ? spin_limit : (1u << 22));
+    g_force_timeout.store(force_timeout);
+}
+
+int read_error_word(const unsigned int *dev_word, unsigned int *out, cudaStream_t st) {
+    // Pageable destination: cudaMemcpyAsync returns once the copy has completed.
+    TL_CUDA_TRY(cudaMemcpyAsync(out, dev_word, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    TL_CUDA_TRY(cudaStreamSynchronize(st));
+    return TL_SUCCESS;
+}
+
+int sync_and_check(cudaStream_t st) {
+    TL_CUDA_TRY(cudaStreamSynchronize(st));
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
+// buildTable: gpu/src/query-mveb.cu:25-47, with the mvEB split of
+// gpu/src/mveb-cycles.cuh:240-247.
+static void build_table(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
+    if (n == 1 || d < 2) return;
+    uint32_t rd, ld;
+    mveb_split(d, rd, ld);
+    uint64_t root_n = low_mask(rd), leaf_n = low_mask(ld);
+    uint32_t i = d - ld;
+    table[i].L = leaf_n;
+    table[i].R = root_n;
+    table[i].D = root_depth;
+    build_table(table, root_n, rd, root_depth);
+    build_table(&table[i], leaf_n, ld, i + root_depth);
+}
+
+// Table-set sizing: gpu/test/query-mveb-fixedN.cu:45-97.
+static void tables_size(uint64_t n, uint32_t &nt, uint32_t &ts, uint32_t &d) {
+    d = bit_length(n);
+    nt = 1;
+    ts = d;
+    if (n == low_mask(d)) return;
+    uint64_t tn = n;
+    uint32_t td = d;
+    while (td >= 2) {
+        uint32_t rd, ld;
+        mveb_split(td, rd, ld);
+        uint64_t r = low_mask(rd), l = low_mask(ld);
+        uint64_t nf = (tn - r) / l, inc = tn - r - nf * l;
+        if (inc == 0) break;
+        uint32_t id = bit_length(inc);
+        ++nt;
+        ts += id;
+        tn = inc;
+        td = id;
+        if (tn == low_mask(id)) break;
+    }
+}
+
+}  // namespace tl
+
+using namespace tl;
+
+static inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+extern "C" {
+
+int tl_version(void) { return TL_VERSION; }
+
+const char *tl_status_string(int status) {
+    switch (status) {
+        case TL_SUCCESS: return "success";
+        case TL_ERROR_INVALID_VALUE: return "invalid value";
+        case TL_ERROR_CUDA: return "CUDA runtime error";
+        case TL_ERROR_TIMEOUT: return "bounded device wait expired";
+        case TL_ERROR_OUT_OF_MEMORY: return "out of device memory";
+        case TL_ERROR_WORKSPACE_TOO_SMALL: return "workspace too small";
+        case TL_ERROR_UNSUPPORTED: return "unsupported size or parameter";
+        default: return "unknown status";
+    }
+}
+
+int tl_last_cuda_error(void) { return t_last_cuda_error; }
+
+// Test hook: bound every device wait to `spin_limit` iterations and, when
+// force_timeout is set, make the waits expect a flag value no tile publishes.
+int tl_debug_set_wait(unsigned int spin_limit, int force_timeout) {
+    debug_set_wait(spin_limit, force_timeout);
+    return TL_SUCCESS;
+}
+
+// Test hook: host replay of the permutation's tile schedule (see emulate_permute).
+int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations) {
+    if (n > 0 && !host_A) return TL_ERROR_INVALID_VALUE;
+    return emulate_permute(layout, n, b, host_A, violations);
+}
+
+int tl_layout_position(int layout, uint64_t n, uint64_t b, uint64_t rank, uint64_t *pos) {
+    if (!pos || rank >= n) return TL_ERROR_INVALID_VALUE;
+    if (layout == TL_LAYOUT_MVEB) {
+        *pos = mveb_pos(n, rank);
+        return TL_SUCCESS;
+    }
+    if (layout == TL_LAYOUT_BST) b = 1;
+    if (layout != TL_LAYOUT_BTREE && layout != TL_LAYOUT_BST) return TL_ERROR_INVALID_VALUE;
+    if (b == 0) return TL_ERROR_INVALID_VALUE;
+    BtreeGeom g = make_btree_geom(n, b);
+    FastDiv64 fd(b + 1);
+    *pos = btree_pos(g, fd, rank);
+    return TL_SUCCESS;
+}
+
+int tl_permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes) {
+    return permute_workspace_bytes(layout, n, b, key_bytes, bytes);
+}
+
+int tl_permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_workspace,
+               uint64_t workspace_bytes, void *stream, float *ms) {
+    return permute(layout, dev_A, n, b, key_bytes, dev_workspace, workspace_bytes, S(stream), ms);
+}
+
+int tl_permute_bst_u32(uint32_t *A, uint64_t n, void *s, float *ms) {
+    return permute(TL_LAYOUT_BST, A, n, 1, 4, nullptr, 0, S(s), ms);
+}
+int tl_permute_bst_u64(uint64_t *A, uint64_t n, void *s, float *ms) {
+    return permute(TL_LAYOUT_BST, A, n, 1, 8, nullptr, 0, S(s), ms);
+}
+int tl_permute_btree_u32(uint32_t *A, uint64_t n, uint64_t b, void *s, float *ms) {
+    return permute(TL_LAYOUT_BTREE, A, n, b, 4, nullptr, 0, S(s), ms);
+}
+int tl_permute_btree_u64(uint64_t *A, uint64_t n, uint64_t b, void *s, float *ms) {
+    return permute(TL_LAYOUT_BTREE, A, n, b, 8, nullptr, 0, S(s), ms);
+}
+int tl_permute_mveb_u32(uint32_t *A, uint64_t n, void *s, float *ms) {
+    return permute(TL_LAYOUT_MVEB, A, n, 0, 4, nullptr, 0, S(s), ms);
+}
+int tl_permute_mveb_u64(uint64_t *A, uint64_t n, void *s, float *ms) {
+    return permute(TL_LAYOUT_MVEB, A, n, 0, 8, nullptr, 0, S(s), ms);
+}
+
+void tl_build_table(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
+    if (table) build_table(table, n, d, root_depth);
+}
+
+int tl_veb_tables_size(uint64_t n, uint32_t *num_tables, uint32_t *table_size, uint32_t *d) {
+    if (n == 0 || !num_tables || !table_size) return TL_ERROR_INVALID_VALUE;
+    uint32_t nt, ts, dd;
+    tables_size(n, nt, ts, dd);
+    *num_tables = nt;
+    *table_size = ts;
+    if (d) *d = dd;
+    return TL_SUCCESS;
+}
+
+// Table-set construction: gpu/test/query-mveb-fixedN.cu:130-165.
+int tl_build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx) {
+    if (n == 0 || !tables || !idx || !table_idx) return TL_ERROR_INVALID_VALUE;
+    uint32_t nt, ts, d;
+    tables_size(n, nt, ts, d);
+    memset(tables, 0, ts * sizeof(tl_veb_table));
+    build_table(tables, n, d, 0);
+    idx[nt - 1] = n;
+    table_idx[0] = 0;
+    uint64_t tn = n;
+    uint32_t td = d;
+    for (uint32_t i = 1; i < nt; ++i) {
+        table_idx[i] = table_idx[i - 1] + td;
+        uint32_t rd, ld;
+        mveb_split(td, rd, ld);
+        uint64_t r = low_mask(rd), l = low_mask(ld);
+        uint64_t nf = (tn - r) / l, inc = tn - r - nf * l;
+        uint32_t id = bit_length(inc);
+        build_table(&tables[table_idx[i]], inc, id, 0);
+        idx[i - 1] = n - inc;
+        tn = inc;
+        td = id;
+    }
+    return TL_SUCCESS;
+}
+
+#define TL_Q(NAME, K, KB, LAYOUT, ...)                                                                  \
+    int NAME {                                                                                          \
+        QueryArgs a{};                                                                                  \
+        a.layout = LAYOUT;                                                                              \
+        a.key_bytes = KB;                                                                               \
+        __VA_ARGS__;                                                                                    \
+        return query(a, S(stream), ms);                                                                 \
+    }
+
+TL_Q(tl_query_bst_u32(const uint32_t *L, uint64_t n, const uint32_t *Q, uint64_t q, uint64_t *ans, void *stream,
+                      float *ms),
+     uint32_t, 4, Q_BST, a.layout_keys = L; a.n = n; a.queries = Q; a.q = q; a.answers = ans)
+TL_Q(tl_query_bst_u64(const uint64_t *L, uint64_t n, const uint64_t *Q, uint64_t q, uint64_t *ans, void *stream,
+                      float *ms),
+     uint64_t, 8, Q_BST, a.layout_keys = L; a.n = n; a.queries = Q; a.q = q; a.answers = ans)
+TL_Q(tl_query_btree_u32(const uint32_t *L, uint64_t n, uint64_t b, const uint32_t *Q, uint64_t q, uint64_t *ans,
+                        void *stream, float *ms),
+     uint32_t, 4, Q_BTREE, a.layout_keys = L; a.n = n; a.b = b; a.queries = Q; a.q = q; a.answers = ans)
+TL_Q(tl_query_btree_u64(const uint64_t *L, uint64_t n, uint64_t b, const uint64_t *Q, uint64_t q, uint64_t *ans,
+                        void *stream, float *ms),
+     uint64_t, 8, Q_BTREE, a.layout_keys = L; a.n = n; a.b = b; a.queries = Q; a.q = q; a.answers = ans)
+TL_Q(tl_query_veb_u32(const uint32_t *L, const tl_veb_table *T, uint64_t n, uint32_t d, const uint32_t *Q,
+                      uint64_t q, uint64_t *ans, void *stream, float *ms),
+     uint32_t, 4, Q_VEB, a.layout_keys = L; a.tables = T; a.n = n; a.d = d; a.queries = Q; a.q = q;
+     a.answers = ans)
+TL_Q(tl_query_veb_u64(const uint64_t *L, const tl_veb_table *T, uint64_t n, uint32_t d, const uint64_t *Q,
+                      uint64_t q, uint64_t *ans, void *stream, float *ms),
+     uint64_t, 8, Q_VEB, a.layout_keys = L; a.tables = T; a.n = n; a.d = d; a.queries = Q; a.q = q;
+     a.answers = ans)
+TL_Q(tl_query_veb_nonperfect_u32(const uint32_t *L, const tl_veb_table *T, const uint64_t *idx,
+                                 const uint32_t *tidx, uint64_t n, uint32_t d, uint32_t nt, const uint32_t *Q,
+                                 uint64_t q, uint64_t *ans, void *stream, float *ms),
+     uint32_t, 4, Q_VEB_NP, a.layout_keys = L; a.tables = T; a.idx = idx; a.table_idx = tidx; a.n = n; a.d = d;
+     a.num_tables = nt; a.queries = Q; a.q = q; a.answers = ans)
+TL_Q(tl_query_veb_nonperfect_u64(const uint64_t *L, const tl_veb_table *T, const uint64_t *idx,
+                                 const uint32_t *tidx, uint64_t n, uint32_t d, uint32_t nt, const uint64_t *Q,
+                                 uint64_t q, uint64_t *ans, void *stream, float *ms),
+     uint64_t, 8, Q_VEB_NP, a.layout_keys = L; a.tables = T; a.idx = idx; a.table_idx = tidx; a.n = n; a.d = d;
+     a.num_tables = nt; a.queries = Q; a.q = q; a.answers = ans)
+
+}  // extern "C"

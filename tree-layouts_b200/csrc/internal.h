@@ -1,0 +1,88 @@
+// Host-side helpers shared by the library's translation units.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/tree_layouts.h"
+
+namespace tl {
+
+void record_cuda_error(cudaError_t e);
+
+#define TL_CUDA_TRY(expr)                       \
+    do {                                        \
+        cudaError_t tl_e_ = (expr);             \
+        if (tl_e_ != cudaSuccess) {             \
+            ::tl::record_cuda_error(tl_e_);     \
+            return TL_ERROR_CUDA;               \
+        }                                       \
+    } while (0)
+
+// Bounded-wait knobs (fault-injection tests shrink the bound and make waits miss).
+unsigned int debug_spin_limit();
+bool debug_force_timeout();
+void debug_set_wait(unsigned int spin_limit, int force_timeout);
+
+// Optional device-time measurement on a stream with CUDA events.
+class EventTimer {
+   public:
+    EventTimer(bool on, cudaStream_t st) : on_(on), st_(st) {
+        if (on_) {
+            cudaEventCreate(&a_);
+            cudaEventCreate(&b_);
+        }
+    }
+    ~EventTimer() {
+        if (on_) {
+            cudaEventDestroy(a_);
+            cudaEventDestroy(b_);
+        }
+    }
+    void start() {
+        if (on_) cudaEventRecord(a_, st_);
+    }
+    void stop() {
+        if (on_) cudaEventRecord(b_, st_);
+    }
+    float elapsed() {
+        float ms = 0.f;
+        if (on_) {
+            cudaEventSynchronize(b_);
+            cudaEventElapsedTime(&ms, a_, b_);
+        }
+        return ms;
+    }
+
+   private:
+    bool on_;
+    cudaStream_t st_;
+    cudaEvent_t a_{}, b_{};
+};
+
+// Reads a device word written by the preceding work on `st` (blocks the host).
+int read_error_word(const unsigned int *dev_word, unsigned int *out, cudaStream_t st);
+int sync_and_check(cudaStream_t st);
+
+int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
+int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations);
+int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
+            uint64_t ws_bytes, cudaStream_t st, float *ms);
+
+enum QueryLayout { Q_BST = 0, Q_BTREE = 1, Q_VEB = 2, Q_VEB_NP = 3 };
+struct QueryArgs {
+    int layout;
+    uint32_t key_bytes;
+    const void *layout_keys;
+    uint64_t n, b;
+    const tl_veb_table *tables;
+    const uint64_t *idx;
+    const uint32_t *table_idx;
+    uint32_t d, num_tables;
+    const void *queries;
+    uint64_t q;
+    uint64_t *answers;
+};
+int query(const QueryArgs &a, cudaStream_t st, float *ms);
+
+}  // namespace tl

@@ -1,0 +1,318 @@
+// Batched exact point queries over the three layouts (sm_100a).
+//
+// Each kernel is persistent (grid = SMs x resident CTAs) and walks the query
+// array with a grid stride.  The first P positions of the layout - the top
+// levels for every layout, since each one stores its root region first - are
+// copied once per CTA into shared memory, so the first levels of every descent
+// cost a shared-memory load instead of an L2/HBM round trip.
+//
+// Answers are the layout position of the key or n (gpu/src/query-bst.cuh:41,
+// gpu/src/query-btree.cuh:59, gpu/src/query-mveb.cuh:65).  For keys present in
+// the layout the descent visits the same nodes as the reference's searches.
+#include <algorithm>
+
+#include "internal.h"
+#include "tl_common.cuh"
+
+namespace tl {
+
+constexpr int kQueryThreads = 256;
+constexpr uint32_t kPinBytes = 48 * 1024;
+
+template <typename K>
+__device__ __forceinline__ void pin_prefix(const K *__restrict__ A, uint64_t P, K *sm) {
+    for (uint64_t x = threadIdx.x; x < P; x += blockDim.x) sm[x] = __ldg(A + x);
+    __syncthreads();
+}
+
+template <typename K>
+__device__ __forceinline__ K key_at(const K *__restrict__ A, const K *sm, uint64_t P, uint64_t i) {
+    return i < P ? sm[i] : __ldg(A + i);
+}
+
+// ---------------------------------------------------------------- BST
+// searchBST (gpu/src/query-bst.cuh:31-42): i = 2i + 1 + (q > A[i]).
+template <typename K>
+__global__ void __launch_bounds__(kQueryThreads)
+bst_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, const K *__restrict__ Q, uint64_t nq,
+                 uint64_t *__restrict__ ans) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *sm = reinterpret_cast<K *>(smem_raw);
+    pin_prefix(A, P, sm);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
+        const K q = __ldcs(Q + qi);
+        uint64_t i = 0, res = n;
+        while (i < n) {
+            const K cur = key_at(A, sm, P, i);
+            if (q == cur) {
+                res = i;
+                break;
+            }
+            i = 2 * i + 1 + (q > cur);
+        }
+        __stcs(ans + qi, res);
+    }
+}
+
+// ---------------------------------------------------------------- B-tree
+// searchBtree (cpu/src/query-btree.h:33-54): the child followed is the number of
+// node keys smaller than the query; an equal key ends the search.  A group of G
+// lanes reads one node cooperatively: lane j of the group owns node slots
+// j, j+G, ...; slots at or past n (the partial last leaf) count as +infinity.
+template <typename K, int G>
+__global__ void __launch_bounds__(kQueryThreads)
+btree_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_t P, const K *__restrict__ Q,
+                   uint64_t nq, uint64_t *__restrict__ ans) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *sm = reinterpret_cast<K *>(smem_raw);
+    pin_prefix(A, P, sm);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t gl = lane % G;                      // lane within the group
+    const uint32_t gbase = lane - gl;                  // first lane of the group
+    const unsigned gmask = (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1)) << gbase;
+    const uint64_t groups = (uint64_t)gridDim.x * blockDim.x / G;
+    const uint64_t gid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint64_t rounds = (nq + groups - 1) / groups;  // uniform trip count keeps warps converged
+    for (uint64_t rd = 0; rd < rounds; ++rd) {
+        const uint64_t qi = rd * groups + gid;
+        const bool active = qi < nq;
+        const K q = active ? Q[qi] : K(0);
+        uint64_t i = 0, res = n;
+        bool done = !active;
+        while (__any_sync(0xFFFFFFFFu, !done)) {
+            if (!done && i >= n) done = true;
+            uint32_t lt = 0;
+            int eq_slot = -1;
+            if (!done) {
+                for (uint64_t s = gl; s < b; s += G) {
+                    const uint64_t p = i + s;
+                    if (p < n) {
+                        const K cur = key_at(A, sm, P, p);
+                        lt += cur < q;
+                        if (cur == q && eq_slot < 0) eq_slot = (int)s;
+                    }
+                }
+            }
+            // group reductions (all 32 lanes take part; inactive lanes add zero)
+            for (int off = G / 2; off > 0; off >>= 1) {
+                lt += __shfl_xor_sync(0xFFFFFFFFu, lt, off);
+                const int o = __shfl_xor_sync(0xFFFFFFFFu, eq_slot, off);
+                if (o >= 0 && (eq_slot < 0 || o < eq_slot)) eq_slot = o;
+            }
+            (void)gmask;
+            if (!done) {
+                // The reference returns the first equal key of the node whose
+                // preceding keys are all smaller; with sorted nodes that is the
+                // equal key at slot lt.
+                if (eq_slot >= 0 && (uint64_t)eq_slot == lt) {
+                    res = i + (uint64_t)eq_slot;
+                    done = true;
+                } else {
+                    i = (i + 1) * (b + 1) + lt * b - 1;
+                }
+            }
+        }
+        if (active && gl == 0) ans[qi] = res;
+    }
+}
+
+// ---------------------------------------------------------------- mvEB
+// searchvEB (gpu/src/query-mveb.cuh:43-66): BFS index i and the table recurrence
+// pos[d] = pos[D_d] + R_d + (i & R_d) * L_d, with pos[] in shared memory, one
+// column per thread (32-bit entries when n < 2^32).  Tables are read through the
+// read-only cache.  A descent past the deepest level ends as "absent" (the
+// reference reads past its table there; it only ever issues hits).
+constexpr int kVebThreads = 128;
+
+template <typename K, typename PosT>
+__device__ __forceinline__ uint64_t veb_descend(const K *__restrict__ A, const K *sm, uint64_t P,
+                                               const tl_veb_table *__restrict__ tab, uint32_t d, K q,
+                                               uint64_t offset, uint64_t limit, PosT *pos, bool &fell) {
+    const uint32_t T = blockDim.x, tid = threadIdx.x;
+    uint32_t cd = 0;
+    uint64_t i = 1, index = 0;
+    pos[tid] = 1;
+    fell = false;
+    while (index + offset < limit) {
+        const K cur = key_at(A, sm, P, offset + index);
+        if (q == cur) return offset + index;
+        if (cd + 1 >= d) {
+            fell = true;
+            return ~0ull;
+        }
+        i = 2 * i + (q > cur);
+        ++cd;
+        const uint64_t L = __ldg(&tab[cd].L), R = __ldg(&tab[cd].R);
+        const uint32_t D = __ldg(&tab[cd].D);
+        const uint64_t p = (uint64_t)pos[tid + T * D] + R + (i & R) * L;
+        pos[tid + T * cd] = (PosT)p;
+        index = p - 1;
+    }
+    return ~0ull;
+}
+
+// idx == nullptr: perfect layout, one table (timeQueryvEB); otherwise the
+// non-perfect table set (timeQueryvEB_nonperfect).
+template <typename K, typename PosT>
+__global__ void __launch_bounds__(kVebThreads)
+veb_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, uint32_t dmax,
+                 const tl_veb_table *__restrict__ tables, const uint64_t *__restrict__ idx,
+                 const uint32_t *__restrict__ table_idx, uint32_t num_tables, const K *__restrict__ Q,
+                 uint64_t nq, uint64_t *__restrict__ ans) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PosT *pos = reinterpret_cast<PosT *>(smem_raw);
+    K *sm = reinterpret_cast<K *>(smem_raw + ((size_t)dmax * blockDim.x * sizeof(PosT) + 15) / 16 * 16);
+    pin_prefix(A, P, sm);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
+        const K q = __ldcs(Q + qi);
+        uint64_t res = n;
+        if (!idx) {
+            bool fell;
+            const uint64_t r = veb_descend<K, PosT>(A, sm, P, tables, bit_length(n), q, 0, n, pos, fell);
+            if (r != ~0ull) res = r;
+        } else {
+            uint64_t offset = 0;
+            for (uint32_t j = 0; j < num_tables; ++j) {
+                const uint32_t dj = bit_length(n - offset);
+                const uint64_t lim = __ldg(idx + j);
+                bool fell;
+                const uint64_t r = veb_descend<K, PosT>(A, sm, P, tables + __ldg(table_idx + j), dj, q, offset,
+                                                        lim, pos, fell);
+                if (r != ~0ull) {
+                    res = r;
+                    break;
+                }
+                if (fell) break;
+                offset = lim;
+            }
+        }
+        __stcs(ans + qi, res);
+    }
+}
+
+// ---------------------------------------------------------------- host
+static int g_qsm = 0;
+static int query_sm_count() {
+    if (!g_qsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_qsm, cudaDevAttrMultiProcessorCount, dev);
+        if (g_qsm <= 0) g_qsm = 148;
+    }
+    return g_qsm;
+}
+
+template <typename Kern>
+static int persistent_grid(Kern kern, size_t smem, uint64_t work_threads, unsigned *grid) {
+    TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kQueryThreads, smem));
+    uint64_t g = (uint64_t)std::max(per_sm, 1) * query_sm_count();
+    uint64_t need = (work_threads + kQueryThreads - 1) / kQueryThreads;
+    *grid = (unsigned)std::max<uint64_t>(1, std::min(g, need));
+    return TL_SUCCESS;
+}
+
+template <typename K>
+static int launch_query(const QueryArgs &a, cudaStream_t st) {
+    const K *A = static_cast<const K *>(a.layout_keys);
+    const K *Q = static_cast<const K *>(a.queries);
+    uint64_t P = std::min<uint64_t>(a.n, kPinBytes / sizeof(K));
+    unsigned grid = 1;
+    if (a.layout == Q_BST) {
+        // whole top levels: 2^T - 1 keys
+        uint64_t top = 1;
+        while (top * 2 + 1 <= P) top = top * 2 + 1;
+        P = std::min<uint64_t>(top, a.n);
+        size_t smem = P * sizeof(K);
+        auto kern = bst_query_kernel<K>;
+        int rc = persistent_grid(kern, smem, a.q, &grid);
+        if (rc) return rc;
+        kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, P, Q, a.q, a.answers);
+    } else if (a.layout == Q_BTREE) {
+        uint64_t top = 0, lvl = a.b;
+        while (top + lvl <= P) {  // whole top levels: (b+1)^L - 1 keys
+            top += lvl;
+            if (lvl > UINT64_MAX / (a.b + 1)) break;
+            lvl *= a.b + 1;
+        }
+        P = std::min<uint64_t>(top, a.n);
+        size_t smem = P * sizeof(K);
+        int G = 1;
+        while (G < 32 && (uint64_t)G < a.b) G <<= 1;
+        int rc = TL_SUCCESS;
+#define TL_BT(GG)                                                                          \
+    case GG: {                                                                             \
+        auto kern = btree_query_kernel<K, GG>;                                             \
+        rc = persistent_grid(kern, smem, a.q * GG, &grid);                                 \
+        if (rc) return rc;                                                                 \
+        kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, a.b, P, Q, a.q, a.answers);        \
+        break;                                                                             \
+    }
+        switch (G) {
+            TL_BT(1)
+            TL_BT(2)
+            TL_BT(4)
+            TL_BT(8)
+            TL_BT(16)
+            TL_BT(32)
+        }
+#undef TL_BT
+    } else {
+        const uint32_t dmax = bit_length(a.n);
+        if (dmax > 63) return TL_ERROR_UNSUPPORTED;
+        const bool np = a.layout == Q_VEB_NP;
+        const bool narrow = a.n < (1ull << 32);
+        const size_t pos_bytes = (size_t)dmax * kVebThreads * (narrow ? 4 : 8);
+        P = std::min<uint64_t>(a.n, (kPinBytes - std::min<size_t>(pos_bytes, kPinBytes / 2)) / sizeof(K));
+        const size_t smem = (pos_bytes + 15) / 16 * 16 + P * sizeof(K);
+        auto launch = [&](auto kern) -> int {
+            TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = 0;
+            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kVebThreads, smem));
+            uint64_t g = (uint64_t)std::max(per_sm, 1) * query_sm_count();
+            uint64_t need = (a.q + kVebThreads - 1) / kVebThreads;
+            unsigned gr = (unsigned)std::max<uint64_t>(1, std::min(g, need));
+            kern<<<gr, kVebThreads, smem, st>>>(A, a.n, P, dmax, a.tables, np ? a.idx : nullptr,
+                                                np ? a.table_idx : nullptr, np ? a.num_tables : 1u, Q, a.q,
+                                                a.answers);
+            return TL_SUCCESS;
+        };
+        int rc = narrow ? launch(veb_query_kernel<K, uint32_t>) : launch(veb_query_kernel<K, uint64_t>);
+        if (rc) return rc;
+    }
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
+int query(const QueryArgs &a, cudaStream_t st, float *ms) {
+    if (a.q == 0) {
+        if (ms) *ms = 0.f;
+        return TL_SUCCESS;
+    }
+    if (!a.queries || !a.answers) return TL_ERROR_INVALID_VALUE;
+    if (a.n == 0) {
+        TL_CUDA_TRY(cudaMemsetAsync(a.answers, 0, a.q * sizeof(uint64_t), st));
+        if (ms) *ms = 0.f;
+        return sync_and_check(st);
+    }
+    if (!a.layout_keys) return TL_ERROR_INVALID_VALUE;
+    if (a.layout == Q_BTREE && a.b == 0) return TL_ERROR_INVALID_VALUE;
+    if ((a.layout == Q_VEB || a.layout == Q_VEB_NP) && !a.tables) return TL_ERROR_INVALID_VALUE;
+    if (a.layout == Q_VEB_NP && (!a.idx || !a.table_idx || a.num_tables == 0)) return TL_ERROR_INVALID_VALUE;
+    EventTimer timer(ms != nullptr, st);
+    timer.start();
+    int rc = a.key_bytes == 8 ? launch_query<uint64_t>(a, st) : launch_query<uint32_t>(a, st);
+    timer.stop();
+    if (rc) return rc;
+    if (ms) {
+        rc = sync_and_check(st);
+        if (rc) return rc;
+        *ms = timer.elapsed();
+    }
+    return TL_SUCCESS;
+}
+
+}  // namespace tl

@@ -1,0 +1,101 @@
+// Building blocks of the in-place streaming permutation: the per-launch control
+// block, tile tickets, read-done flags with bounded waits, and the tile loader.
+//
+// The in-place pass walks the array one tile at a time.  Tiles are handed out by
+// an atomic ticket counter, so a CTA holding ticket t knows every ticket below t
+// is already owned by a running CTA.  A CTA first copies its whole source tile
+// into shared memory and then publishes "tile read" (release).  Before storing,
+// it waits (acquire) for the flags of the tiles whose source overlaps the
+// destinations it will write.  Those tiles always hold smaller tickets, and a
+// CTA publishes its flag before it waits on anything, so every wait ends.  Waits
+// are still bounded: on expiry the CTA records TL_ERROR_TIMEOUT in the control
+// block, skips its stores, and the host reports the error.
+#pragma once
+
+#include "tl_common.cuh"
+
+namespace tl {
+
+struct Ctrl {
+    unsigned long long ticket;
+    unsigned int error;
+    unsigned int flag_value;      // value a tile publishes once its source is read
+    unsigned int wait_value;      // value a wait expects (== flag_value except in fault tests)
+    unsigned int spin_limit;      // iterations of a bounded wait (x ~256 ns each)
+    unsigned int pad[10];
+};
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned int *p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits until flag == want; false (and the error recorded) if the bound expires.
+__device__ __forceinline__ bool wait_flag(const unsigned int *flag, unsigned int want, Ctrl *ctrl) {
+    unsigned int limit = ctrl->spin_limit;
+    unsigned int ns = 32;
+    for (unsigned int it = 0; it <= limit; ++it) {
+        if (ld_acquire(flag) == want) return true;
+        __nanosleep(ns);
+        if (ns < 256) ns <<= 1;
+    }
+    atomicOr(&ctrl->error, 1u << TL_ERROR_TIMEOUT);
+    return false;
+}
+
+// Block-wide: fetch the next ticket (same value in every thread).
+__device__ __forceinline__ unsigned long long next_ticket(Ctrl *ctrl, unsigned long long *s_ticket) {
+    __syncthreads();
+    if (threadIdx.x == 0) *s_ticket = atomicAdd(&ctrl->ticket, 1ull);
+    __syncthreads();
+    return *s_ticket;
+}
+
+// Block-wide: publish that this tile's source has been read into shared memory.
+__device__ __forceinline__ void publish_read(unsigned int *flag, Ctrl *ctrl) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        st_release(flag, ctrl->flag_value);
+    }
+}
+
+// Block-wide: wait for tiles [k_lo, k_hi] (inclusive, global tile ids) to be read.
+// Returns true when all were seen before the bound expired.
+__device__ __forceinline__ bool wait_tiles(const unsigned int *flags, long long k_lo, long long k_hi,
+                                           Ctrl *ctrl, int *s_ok) {
+    if (threadIdx.x == 0) *s_ok = 1;
+    __syncthreads();
+    for (long long k = k_lo + threadIdx.x; k <= k_hi; k += blockDim.x)
+        if (!wait_flag(&flags[k], ctrl->wait_value, ctrl)) *s_ok = 0;
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// Copies src[p0, p1) into shared memory so that element x sits at
+// sm[x - base], base = p0 rounded down to a 16-byte boundary of the global
+// address.  Returns base.  Interior 16-byte chunks use vector loads.
+template <typename K>
+__device__ __forceinline__ uint64_t load_tile(const K *__restrict__ src, uint64_t p0, uint64_t p1, K *sm) {
+    constexpr uint32_t V = 16 / sizeof(K);
+    uintptr_t addr0 = reinterpret_cast<uintptr_t>(src + p0);
+    uint64_t head = (addr0 & 15) / sizeof(K);  // elements before the 16-byte boundary
+    uint64_t base = p0 - head;
+    uint64_t a0 = head ? p0 + (V - head) : p0;  // first aligned element
+    if (a0 > p1) a0 = p1;
+    uint64_t nvec = (p1 - a0) / V;
+    uint64_t a1 = a0 + nvec * V;
+    for (uint64_t x = p0 + threadIdx.x; x < a0; x += blockDim.x) sm[x - base] = src[x];
+    const uint4 *vsrc = reinterpret_cast<const uint4 *>(src + a0);
+    uint4 *vdst = reinterpret_cast<uint4 *>(sm + (a0 - base));
+    for (uint64_t v = threadIdx.x; v < nvec; v += blockDim.x) vdst[v] = __ldcs(vsrc + v);
+    for (uint64_t x = a1 + threadIdx.x; x < p1; x += blockDim.x) sm[x - base] = src[x];
+    return base;
+}
+
+}  // namespace tl
