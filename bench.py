@@ -1,0 +1,359 @@
+#!/usr/bin/env python3
+"""Benchmark of the tree-layout hot path on B200.
+
+Default workload (the configuration the headline metric is quoted on): in-place
+permutation of n = 500,000,000 sorted uint64 keys (prefix sums of uniform gaps
+in [1,16], seed 3) into a level-order B-tree with b = 16 keys per node, then
+q = 2^27 point queries (seed 4, 50% hits / 50% uniform in [min, max]).
+
+One step = one permutation of the full array.  Between steps the array is
+restored from a pristine sorted copy (untimed, like the reference drivers'
+re-initialisation); the 4 GB input is far larger than the 126 MB L2, so no
+extra flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  Multi-GPU (torchrun): every rank permutes its
+own replica (a single array's permutation does not shard), value = all ranks'
+bytes / max-over-ranks time ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tree-layouts_b200"))
+
+WORKLOADS = {
+    # name: (layout, b, n, key_bytes, gap_hi, key seed, q, query seed)
+    "btree-b16-n500M-u64": ("btree", 16, 500_000_000, 8, 16, 3, 2**27, 4),
+    "btree-b16-n2^30-u64": ("btree", 16, 2**30, 8, 16, 8, 2**27, 9),
+    "mveb-n2^30-1-u32": ("mveb", 0, 2**30 - 1, 4, 3, 5, 2**27, 6),
+    "mveb-n300M-u32": ("mveb", 0, 300_000_000, 4, 3, 5, 2**27, 6),
+    "bst-n2^30-1-u64": ("bst", 1, 2**30 - 1, 8, 16, 1, 2**27, 2),
+    "bst-n2^20-1-u64": ("bst", 1, 2**20 - 1, 8, 16, 1, 2**20, 2),
+}
+DEFAULT = "btree-b16-n500M-u64"
+METRIC = "permute GB/s (2*n*key_bytes / device time), in-place sorted -> level-order B-tree"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = os.path.join("/tmp", f"tl_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_permute(layout, b, n_sample, key_bytes, reps, min_seconds=8.0):
+    """The reference's own CPU OpenMP permutation (compiled from its sources into
+    oracle/_ref/libref_cpu.so) on n_sample keys with every host thread; falls back
+    to the oracle's single-thread C restatement when that build is absent."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = os.cpu_count() or 1
+    ref = O.ref_cpu()
+    A = np.empty(n_sample, dtype=np.uint64)
+    times = []
+    t_begin = time.time()
+    kind = "reference" if ref is not None else "port"
+    for r in range(reps):
+        A[:] = np.arange(1, n_sample + 1, dtype=np.uint64)  # initSortedList (untimed)
+        if ref is not None:
+            if layout == "bst":
+                ms = ref.ref_cpu_permute_bst_u64(A, n_sample, threads)
+            else:
+                ms = ref.ref_cpu_permute_btree_u64(A, n_sample, b, threads)
+        else:
+            threads = 1
+            ms = O.lib().orc_time_permute_btree(A, n_sample, b if layout != "bst" else 1)
+        times.append(ms)
+        if time.time() - t_begin > min_seconds and r >= 1:
+            break
+    ms = statistics.median(times)
+    gbs = 2.0 * n_sample * key_bytes / (ms * 1e-3) / 1e9
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": f"{layout} b={b} n={n_sample} uint64 keys 1..n (initSortedList), median of {len(times)} "
+                      f"runs of timePermuteBtree on {threads} threads ({ms:.1f} ms)"}
+
+
+def run_reference(args, rank):
+    layout, b, n, kb, *_ = WORKLOADS[args.workload]
+    if rank != 0:
+        return
+    if layout == "mveb":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU code has no mvEB layout "
+                          "(cpu/src builds the standard vEB); its mvEB exists only as GPU code"}))
+        return
+    n_sample = min(n, args.cpu_sample)
+    steps = []
+    for _ in range(args.warmup):
+        cpu_reference_permute(layout, b, n_sample, kb, 1, 0)
+    for _ in range(args.steps):
+        steps.append(cpu_reference_permute(layout, b, n_sample, kb, 1, 0))
+    vals = [s["value"] for s in steps]
+    v = statistics.median(vals)
+    ms = 2.0 * n_sample * 8 / (v * 1e9) * 1e3
+    cb = dict(steps[0])
+    cb["value"] = v
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "b": b, "key_bytes": kb, "sample_n": n_sample,
+                   "note": "reference CPU OpenMP timePermuteBtree (cpu/src/btree-cycles.h) on the host cores"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    import tree_layouts as T
+    from tree_layouts import data
+
+    layout, b, n, kb, gap_hi, kseed, q, qseed = WORKLOADS[args.workload]
+    if args.n:
+        n = args.n
+    L = T.lib()
+    L.tl_debug_permute_phases.argtypes = [C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p,
+                                          C.POINTER(C.c_float)]
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    pristine = data.sorted_keys_torch(n, 1, gap_hi, kseed + rank, kb, dev)
+    A = torch.empty_like(pristine)
+    lay = T.LAYOUTS[layout]
+    phases = (C.c_float * 2)()
+
+    def step():
+        A.copy_(pristine)  # re-initialise (untimed)
+        rc = L.tl_debug_permute_phases(lay, A.data_ptr(), n, b or 16, kb, stream.cuda_stream, phases)
+        if rc:
+            raise T.TreeLayoutError(rc, "permute")
+        return phases[0], phases[1]
+
+    for _ in range(args.warmup):
+        step()
+    # correctness spot check of the last warm-up result (sampled positions)
+    rng = np.random.default_rng(0)
+    ranks = rng.integers(0, n, 256)
+    pos = torch.tensor([T.layout_position(layout, n, int(s), b or 16) for s in ranks], device=dev)
+    assert torch.equal(A[pos], pristine[torch.from_numpy(ranks).to(dev)]), "layout spot check failed"
+
+    clocks = ClockSampler(local)
+    barrier(world)
+    clocks.start()
+    t_stream, t_scatter = [], []
+    for _ in range(args.steps):
+        a, c = step()
+        t_stream.append(a)
+        t_scatter.append(c)
+    barrier(world)
+    clk = clocks.stop()
+    step_ms = [a + c for a, c in zip(t_stream, t_scatter)]
+    ms_local = sum(step_ms) / len(step_ms)
+    ms = reduce_max(ms_local, world)
+    bytes_step = 2.0 * n * kb
+    value = world * bytes_step / (ms * 1e-3) / 1e9
+
+    peak, peak_kind = peaks()
+    stream_ms = sum(t_stream) / len(t_stream)
+    achieved = bytes_step / (stream_ms * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"stream_traffic_{args.workload}.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    # plain B-tree / BST / mvEB queries on the permuted layout (device time)
+    qinfo = None
+    if args.queries and q:
+        Q = data.queries_torch(pristine, q, 0.5, qseed)
+        ans = torch.empty(q, dtype=torch.int64, device=dev)
+        tabs = T.VebTablesDevice(n, dev) if layout == "mveb" else None
+        for _ in range(2):
+            T.query(layout, A, Q, ans, b or 16, tables=tabs)
+        qms = []
+        for _ in range(3):
+            qms.append(T.query(layout, A, Q, ans, b or 16, tables=tabs, timed=True))
+        hits = int((ans != n).sum().item())
+        qms_med = statistics.median(qms)
+        qinfo = {"q": q, "ms": round(qms_med, 3), "queries_per_s": round(q / (qms_med * 1e-3), 1),
+                 "hits": hits, "kernel": f"plain {layout} query"}
+        del Q, ans
+
+    # end to end through the C ABI with host buffers: H2D keys, permute, D2H layout
+    e2e = None
+    if args.e2e_steps > 0:
+        host_in = torch.empty(n, dtype=pristine.dtype, pin_memory=True)
+        host_in.copy_(pristine)
+        host_out = torch.empty_like(host_in, pin_memory=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tms = []
+        for i in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            A.copy_(host_in, non_blocking=True)
+            rc = L.tl_permute(lay, C.c_void_p(A.data_ptr()), n, b or 16, kb, None, 0,
+                              C.c_void_p(stream.cuda_stream), None)
+            if rc:
+                raise T.TreeLayoutError(rc, "permute (e2e)")
+            host_out.copy_(A, non_blocking=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i:  # first one warms the pinned path
+                tms.append(e0.elapsed_time(e1))
+        assert torch.equal(host_out[:1024].to(dev), A[:1024])
+        ems = reduce_max(statistics.median(tms), world)
+        e2e = {"value": round(world * bytes_step / (ems * 1e-3) / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": n * kb, "d2h_bytes_per_step": n * kb, "ms_per_step": round(ems, 3)}
+        del host_in, host_out
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_sample > 0 and layout != "mveb":
+        cpu = cpu_reference_permute(layout, b, min(n, args.cpu_sample), kb, 5)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC if layout == "btree" else METRIC.replace("level-order B-tree", layout),
+            "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64" if kb == 8 else "u32", "data": "synthetic",
+            "config": {"workload": args.workload, "layout": layout, "b": b, "n": n, "key_bytes": kb,
+                       "keys": f"prefix sums of uniform gaps in [1,{gap_hi}], seed {kseed}",
+                       "l2": "inputs larger than L2 (no flush needed)",
+                       "restore": "array re-initialised from a pristine copy between steps, untimed",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": f"{layout}_stream_kernel", "achieved": round(achieved, 1),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_source": f"hbm_gbs of {peak_kind}", "traffic": traffic,
+                         "algorithmic_bytes_per_launch": int(bytes_step),
+                         "stream_ms": round(stream_ms, 4), "scatter_ms": round(sum(t_scatter) / len(t_scatter), 4),
+                         "whole_permute_frac": round(bytes_step / (ms_local * 1e-3) / 1e9 / peak, 4)},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "queries": qinfo,
+            "clocks": clk,
+            "gpu_launches": 2 * args.steps,
+        }
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=0, help="override n (profiling runs)")
+    ap.add_argument("--queries", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=50_000_000)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, rank)
+        return
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

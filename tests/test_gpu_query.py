@@ -1,0 +1,66 @@
+"""Parity of the sm_100a query kernels with the oracle (and, through the golden
+fixtures, with the reference's own query code), through the C ABI."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import tree_layouts as T
+from gpu_util import from_dev, to_dev
+from tree_layouts import data
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint64).tobytes()).hexdigest()[:24]
+
+
+def gpu_answers(layout, tree, Q, b=16):
+    import torch
+    ans = torch.empty(len(Q), dtype=torch.int64, device="cuda")
+    T.query(layout, to_dev(tree), to_dev(Q), ans, b)
+    return ans.cpu().numpy().view(np.uint64)
+
+
+@pytest.mark.parametrize("layout,b", [("bst", 1), ("btree", 16), ("btree", 8), ("btree", 3), ("btree", 32),
+                                      ("btree", 1), ("btree", 64), ("mveb", 0)])
+@pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
+def test_queries_match_oracle(layout, b, dtype):
+    for n in [1, 2, 3, 5, 16, 17, 100, 255, 1000, 4097, 65535, 70001, 1048575, 3000017]:
+        keys = data.sorted_keys_np(n, 1, 16 if dtype == np.uint64 else 3, n, dtype)
+        tree = O.permute(layout, keys, b or 16)
+        Q = data.queries_np(keys, 5000, 0.5, n + 1)
+        Q = np.concatenate([Q, keys[:1] - 1 if keys[0] > 0 else keys[:1], keys[-1:] + 1]).astype(dtype)
+        exp = O.search(layout, tree, Q, b or 16)
+        got = gpu_answers(layout, tree, Q, b or 16)
+        assert np.array_equal(got, exp), (layout, b, n)
+
+
+def test_queries_match_reference_golden():
+    with open(os.path.join(GOLD, "golden_cpu.json")) as f:
+        g = json.load(f)
+    for e in g["query_btree"]:
+        keys = data.sorted_keys_np(e["n"], 1, 16, e["seed"])
+        Q = data.queries_np(keys, e["q"], 0.5, e["seed"] + 1)
+        assert sha(gpu_answers("btree", O.permute("btree", keys, e["b"]), Q, e["b"])) == e["sha"]
+    for e in g["query_bst"]:
+        keys = data.sorted_keys_np(e["n"], 1, 16, e["seed"])
+        Q = data.queries_np(keys, e["q"], 0.5, e["seed"] + 1)
+        assert sha(gpu_answers("bst", O.permute("bst", keys), Q)) == e["sha"]
+
+
+def test_benchmark_query_shapes_small():
+    # config shapes at reduced n: BST 2^20-1 u64 with q=2^20, mvEB non-perfect u32 tables
+    keys = data.sorted_keys_np(2**20 - 1, 1, 16, 1)
+    Q = data.queries_np(keys, 2**20, 0.5, 2)
+    tree = O.permute("bst", keys)
+    assert np.array_equal(gpu_answers("bst", tree, Q), O.search("bst", tree, Q))
+    keys = data.sorted_keys_np(3_000_000, 1, 3, 5, np.uint32)
+    Q = data.queries_np(keys, 200_000, 0.5, 6)
+    tree = O.permute("mveb", keys)
+    assert np.array_equal(gpu_answers("mveb", tree, Q), O.search("mveb", tree, Q))

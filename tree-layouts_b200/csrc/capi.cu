@@ -134,6 +134,14 @@ int tl_permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_byt
     return permute(layout, dev_A, n, b, key_bytes, dev_workspace, workspace_bytes, S(stream), ms);
 }
 
+// Profiling hook: tl_permute with device times of its two passes
+// (phase_ms[0]: control setup + stream kernel, phase_ms[1]: scatter kernel).
+int tl_debug_permute_phases(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *stream,
+                            float *phase_ms) {
+    if (!phase_ms) return TL_ERROR_INVALID_VALUE;
+    return permute(layout, dev_A, n, b, key_bytes, nullptr, 0, S(stream), nullptr, phase_ms);
+}
+
 int tl_permute_bst_u32(uint32_t *A, uint64_t n, void *s, float *ms) {
     return permute(TL_LAYOUT_BST, A, n, 1, 4, nullptr, 0, S(s), ms);
 }

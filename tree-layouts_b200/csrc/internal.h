@@ -37,6 +37,7 @@ class EventTimer {
         if (on_) {
             cudaEventDestroy(a_);
             cudaEventDestroy(b_);
+            if (m_) cudaEventDestroy(m_);
         }
     }
     void start() {
@@ -44,6 +45,21 @@ class EventTimer {
     }
     void stop() {
         if (on_) cudaEventRecord(b_, st_);
+    }
+    // Optional split point: elapsed_split() returns [start, mid] and [mid, stop].
+    void mid() {
+        if (on_) {
+            if (!m_) cudaEventCreate(&m_);
+            cudaEventRecord(m_, st_);
+        }
+    }
+    void elapsed_split(float *first, float *second) {
+        *first = *second = 0.f;
+        if (on_ && m_) {
+            cudaEventSynchronize(b_);
+            cudaEventElapsedTime(first, a_, m_);
+            cudaEventElapsedTime(second, m_, b_);
+        }
     }
     float elapsed() {
         float ms = 0.f;
@@ -57,7 +73,7 @@ class EventTimer {
    private:
     bool on_;
     cudaStream_t st_;
-    cudaEvent_t a_{}, b_{};
+    cudaEvent_t a_{}, b_{}, m_{};
 };
 
 // Reads a device word written by the preceding work on `st` (blocks the host).
@@ -67,7 +83,7 @@ int sync_and_check(cudaStream_t st);
 int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
 int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations);
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
-            uint64_t ws_bytes, cudaStream_t st, float *ms);
+            uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms = nullptr);
 
 enum QueryLayout { Q_BST = 0, Q_BTREE = 1, Q_VEB = 2, Q_VEB_NP = 3 };
 struct QueryArgs {

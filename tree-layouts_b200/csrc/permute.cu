@@ -320,7 +320,7 @@ static int sm_count() {
 }
 
 template <typename K>
-static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st) {
+static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st, EventTimer &timer) {
     K *scr = reinterpret_cast<K *>(ws);
     unsigned int *flags = reinterpret_cast<unsigned int *>(ws + pl.off_flags);
     Ctrl *ctrl = reinterpret_cast<Ctrl *>(ws + pl.off_ctrl);
@@ -341,6 +341,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * smx, std::max<uint64_t>(pl.ntiles, 1));
         if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.mp, ctrl, flags);
         TL_CUDA_TRY(cudaGetLastError());
+        timer.mid();
         if (pl.scratch_keys) {
             uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterThreads - 1) / kScatterThreads,
                                              (uint64_t)smx * 8);
@@ -355,6 +356,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * smx, std::max<uint64_t>(pl.ntiles, 1));
         if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, flags);
         TL_CUDA_TRY(cudaGetLastError());
+        timer.mid();
         if (pl.scratch_keys) {
             uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterThreads - 1) / kScatterThreads,
                                              (uint64_t)smx * 8);
@@ -363,6 +365,22 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         }
     }
     return TL_SUCCESS;
+}
+
+// The library's own workspaces come from the device's stream-ordered pool; keep
+// freed blocks in the pool (instead of returning them to the driver at every
+// synchronisation) so repeated calls reuse them without re-mapping memory.
+static void keep_pool_memory() {
+    static std::once_flag once[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::call_once(once[dev], [dev] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    });
 }
 
 int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes) {
@@ -375,8 +393,10 @@ int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_byt
 }
 
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
-            uint64_t ws_bytes, cudaStream_t st, float *ms) {
+            uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms) {
     if (n > 0 && !dev_A) return TL_ERROR_INVALID_VALUE;
+    if (reinterpret_cast<uintptr_t>(dev_A) % (key_bytes ? key_bytes : 1)) return TL_ERROR_INVALID_VALUE;
+    if (dev_ws && reinterpret_cast<uintptr_t>(dev_ws) % 256) return TL_ERROR_INVALID_VALUE;
     PermutePlan pl;
     int rc = make_plan(layout, n, b, key_bytes, pl);
     if (rc) return rc;
@@ -385,10 +405,11 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
         return TL_SUCCESS;
     }
     if (dev_ws && ws_bytes < pl.bytes) return TL_ERROR_WORKSPACE_TOO_SMALL;
-    EventTimer timer(ms != nullptr, st);
+    EventTimer timer(ms != nullptr || phase_ms != nullptr, st);
     char *ws = static_cast<char *>(dev_ws);
     bool owned = false;
     if (!ws) {
+        keep_pool_memory();
         if (cudaMallocAsync(reinterpret_cast<void **>(&ws), pl.bytes, st) != cudaSuccess) {
             record_cuda_error(cudaGetLastError());
             return TL_ERROR_OUT_OF_MEMORY;
@@ -396,8 +417,8 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
         owned = true;
     }
     timer.start();
-    rc = key_bytes == 8 ? launch_permute<uint64_t>(pl, static_cast<uint64_t *>(dev_A), ws, st)
-                        : launch_permute<uint32_t>(pl, static_cast<uint32_t *>(dev_A), ws, st);
+    rc = key_bytes == 8 ? launch_permute<uint64_t>(pl, static_cast<uint64_t *>(dev_A), ws, st, timer)
+                        : launch_permute<uint32_t>(pl, static_cast<uint32_t *>(dev_A), ws, st, timer);
     timer.stop();
     unsigned int err = 0;
     if (rc == TL_SUCCESS) {
@@ -408,6 +429,7 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
     if (rc == TL_SUCCESS) rc = sync_and_check(st);
     if (rc == TL_SUCCESS && err) rc = TL_ERROR_TIMEOUT;
     if (rc == TL_SUCCESS && ms) *ms = timer.elapsed();
+    if (rc == TL_SUCCESS && phase_ms) timer.elapsed_split(&phase_ms[0], &phase_ms[1]);
     return rc;
 }
 
@@ -476,7 +498,10 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
                     for (uint64_t gi = g0; gi < g1; ++gi) {
                         const uint64_t gsrc = R.src + (gi << R.U) - p0;
                         const uint64_t dst = mveb_unit_dst(R, gi);
-                        for (uint64_t q = 0; q < u; ++q) W(dst + q, tile[gsrc + inv[q]]);
+                        for (uint64_t q = 0; q < u; ++q) {
+                            if (gsrc + inv[q] >= p1 - p0) { ++viol; continue; }
+                            W(dst + q, tile[gsrc + inv[q]]);
+                        }
                         if (R.src + (gi << R.U) + u < R.src + R.len) SC(R.slot_base + gi, tile[gsrc + u]);
                     }
                 }

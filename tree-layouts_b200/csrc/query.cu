@@ -108,6 +108,8 @@ btree_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_t P, 
                 if (eq_slot >= 0 && (uint64_t)eq_slot == lt) {
                     res = i + (uint64_t)eq_slot;
                     done = true;
+                } else if (i + 1 > (n + 1) / (b + 1)) {
+                    done = true;  // every child starts past n; also keeps (i+1)(b+1) from overflowing
                 } else {
                     i = (i + 1) * (b + 1) + lt * b - 1;
                 }
@@ -145,6 +147,10 @@ __device__ __forceinline__ uint64_t veb_descend(const K *__restrict__ A, const K
         ++cd;
         const uint64_t L = __ldg(&tab[cd].L), R = __ldg(&tab[cd].R);
         const uint32_t D = __ldg(&tab[cd].D);
+        if (D >= cd) {  // not a table built by buildTable: stop instead of reading outside pos[]
+            fell = true;
+            return ~0ull;
+        }
         const uint64_t p = (uint64_t)pos[tid + T * D] + R + (i & R) * L;
         pos[tid + T * cd] = (PosT)p;
         index = p - 1;
