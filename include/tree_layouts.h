@@ -14,8 +14,11 @@
  *  - dev_* pointers are device (HBM) pointers; host_* pointers are host memory.
  *  - stream: a cudaStream_t passed as void* (NULL = legacy default stream).
  *  - ms: if non-NULL the call synchronises the stream and stores the device time
- *    of the operation in milliseconds (CUDA events on `stream`); if NULL the call
- *    is asynchronous with respect to the host.
+ *    of the operation in milliseconds (CUDA events on `stream`).  Queries with
+ *    ms == NULL are asynchronous with respect to the host.  Permutations always
+ *    return after their work on `stream` has finished: they read back the status
+ *    of their bounded device-side waits (TL_ERROR_TIMEOUT), like the reference's
+ *    timePermute* functions, which end in cudaDeviceSynchronize.
  *  - Keys of a layout must be strictly increasing before a permutation for the
  *    queries to be meaningful; the permutations themselves move words and never
  *    look at key values.
@@ -138,6 +141,23 @@ int tl_query_veb_nonperfect_u64(const uint64_t *dev_layout, const tl_veb_table *
                                 uint64_t n, uint32_t d, uint32_t num_tables,
                                 const uint64_t *dev_queries, uint64_t q, uint64_t *dev_answers,
                                 void *stream, float *ms);
+
+/* ---------------------------------------------------------------- test and profiling hooks */
+/* Bound every device-side wait to spin_limit iterations (0 = default, about one
+ * second) and, when force_timeout != 0, make the waits expect a flag value no
+ * tile publishes, so they expire: exercises TL_ERROR_TIMEOUT without a fault. */
+int tl_debug_set_wait(unsigned int spin_limit, int force_timeout);
+/* Host replay of the permutation's tile schedule on a host array of n 64-bit
+ * words, with the same index helpers as the kernels; *violations counts
+ * protocol breaches (stale read, unguarded store, bad wait, position or scratch
+ * slot not written exactly once). */
+int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations);
+/* Schedule the B-tree permutation uses for (n, b): 0 right-to-left, 1 left-to-right. */
+int tl_debug_btree_plan(uint64_t n, uint64_t b);
+/* tl_permute with library-allocated workspace, reporting the device time of its
+ * two passes: phase_ms[0] = setup + stream kernel, phase_ms[1] = scatter kernel. */
+int tl_debug_permute_phases(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
+                            void *stream, float *phase_ms);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,15 @@ def test_tile_schedule_replay_matches_oracle(layout, b):
         assert np.array_equal(got, exp), (layout, b, n)
 
 
+def test_both_btree_schedules_are_exercised():
+    lib = T.lib()
+    lib.tl_debug_btree_plan.argtypes = [C.c_uint64, C.c_uint64]
+    plans = {lib.tl_debug_btree_plan(n, b) for n in SIZES for b in (2, 3, 8, 16, 31) if n > b}
+    assert plans == {0, 1}
+    assert lib.tl_debug_btree_plan(500_000_000, 16) == 1  # top tree holds 82% of the keys
+    assert lib.tl_debug_btree_plan(2**30, 16) == 0
+
+
 @pytest.mark.parametrize("layout,b", [("bst", 1), ("btree", 16), ("btree", 5), ("mveb", 0)])
 def test_layout_position_matches_oracle(layout, b):
     for n in [1, 2, 3, 16, 17, 100, 4097, 65537, 300001]:

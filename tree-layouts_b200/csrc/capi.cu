@@ -104,6 +104,10 @@ int tl_debug_set_wait(unsigned int spin_limit, int force_timeout) {
     return TL_SUCCESS;
 }
 
+// Test hook: which B-tree schedule the permutation uses (0: right-to-left
+// stream, top tree via scratch; 1: left-to-right stream, last level via scratch).
+int tl_debug_btree_plan(uint64_t n, uint64_t b) { return btree_plan_of(n, b); }
+
 // Test hook: host replay of the permutation's tile schedule (see emulate_permute).
 int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations) {
     if (n > 0 && !host_A) return TL_ERROR_INVALID_VALUE;

@@ -41,42 +41,92 @@ constexpr uint64_t stream_tile_keys() {
 static inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 // ---------------------------------------------------------------- B-tree stream
+// Two schedules.  Plan R (right to left): the last level's keys go straight to
+// their final positions (they move right), the whole top tree goes through
+// scratch.  Plan L (left to right), for trees whose top tree holds most keys:
+// the top tree's own last level goes straight to its final positions (those
+// keys move left), the last level and the upper top levels go through scratch.
+// The host picks the plan with the smaller scratch (the second pass's traffic).
+enum BtreePlan { PLAN_R = 0, PLAN_L = 1 };
+
 struct BtreeStream {
     BtreeGeom g;
     FastDiv64 fd;
     uint64_t tile_keys, ntiles;
+    int plan;
+    uint64_t i2;          // plan L: first position of the top tree's last level, (b+1)^(h-1) - 1
+    uint64_t ibase;       // plan L: floor(i / (b+1))
+    uint64_t nscratch;    // scratch slots
 };
 
-// Source range of tile k (tiles ascend with position; ticket t takes k = ntiles-1-t).
+TL_HD uint64_t btree_tile_of_ticket(const BtreeStream &S, uint64_t t) {
+    return S.plan == PLAN_R ? S.ntiles - 1 - t : t;
+}
+
+// Source range of tile k (tiles ascend with position).
 TL_HD void btree_tile(const BtreeStream &S, uint64_t k, uint64_t &p0, uint64_t &p1) {
     p0 = k * S.tile_keys;
     p1 = p0 + S.tile_keys < S.g.n ? p0 + S.tile_keys : S.g.n;
 }
 
-// Sorted rank -> destination of a bulk (leaf-level) key, extended monotonically
+// Plan R: sorted rank -> destination of a last-level key, extended monotonically
 // over the separators in between; bounds the destinations of a tile.
 TL_HD uint64_t btree_leaf_dest_bound(const BtreeStream &S, uint64_t s) {
     return s < S.g.l + S.g.i ? S.g.ni + s - S.fd.div(s) : S.g.ni + s - S.g.i;
 }
 
-// Tiles (other than k itself) whose source lies under the bulk destinations of
-// tile [p0, p1); all of them lie right of the tile.  False if there are none.
+// Plan L: sorted rank s >= lir (top rank c) -> destination of a key of the top
+// tree's last level, extended monotonically over the upper keys.
+TL_HD uint64_t btree_top_last_dest_bound(const BtreeStream &S, uint64_t s) {
+    const uint64_t c = s - S.g.l - S.g.r;
+    return S.i2 + c - S.fd.div(c + 1);
+}
+
+// Tiles (other than k) whose source lies under the direct destinations of tile
+// [p0, p1): right of the tile for plan R, left of it for plan L, i.e. always
+// tiles with earlier tickets.  False if there are none.
 TL_HD bool btree_tile_wait(const BtreeStream &S, uint64_t p0, uint64_t p1, uint64_t &k_lo, uint64_t &k_hi) {
-    if (p0 >= S.g.lir) return false;
-    uint64_t d0 = btree_leaf_dest_bound(S, p0);
-    uint64_t d1 = btree_leaf_dest_bound(S, (p1 < S.g.lir ? p1 : S.g.lir) - 1) + 1;
-    if (d1 > S.g.n) d1 = S.g.n;  // a trailing separator bounds past the last leaf key
-    uint64_t lo = d0 > p1 ? d0 : p1;
-    if (lo >= d1) return false;
-    k_lo = lo / S.tile_keys;
-    k_hi = (d1 - 1) / S.tile_keys;
+    const BtreeGeom &g = S.g;
+    if (S.plan == PLAN_R) {
+        if (p0 >= g.lir) return false;
+        uint64_t d0 = btree_leaf_dest_bound(S, p0);
+        uint64_t d1 = btree_leaf_dest_bound(S, (p1 < g.lir ? p1 : g.lir) - 1) + 1;
+        if (d1 > g.n) d1 = g.n;  // a trailing separator bounds past the last leaf key
+        uint64_t lo = d0 > p1 ? d0 : p1;
+        if (lo >= d1) return false;
+        k_lo = lo / S.tile_keys;
+        k_hi = (d1 - 1) / S.tile_keys;
+        return true;
+    }
+    if (p1 <= g.lir) return false;
+    uint64_t d0 = btree_top_last_dest_bound(S, p0 > g.lir ? p0 : g.lir);
+    uint64_t d1 = btree_top_last_dest_bound(S, p1 - 1) + 1;
+    uint64_t hi = d1 < p0 ? d1 : p0;
+    if (d0 >= hi) return false;
+    k_lo = d0 / S.tile_keys;
+    k_hi = (hi - 1) / S.tile_keys;
     return true;
 }
 
 // Where sorted rank x goes in the stream pass: true -> A[idx] (final position),
-// false -> scratch[idx] (top rank).
+// false -> scratch[idx].
 TL_HD bool btree_place(const BtreeStream &S, uint64_t x, uint64_t &idx) {
     const BtreeGeom &g = S.g;
+    if (S.plan == PLAN_L) {
+        if (x < g.lir) {
+            idx = x;
+            return false;
+        }
+        const uint64_t c = x - g.l - g.r;
+        uint64_t q, rem;
+        S.fd.divmod(c + 1, q, rem);
+        if (rem != 0) {
+            idx = S.i2 + c - q;
+            return true;
+        }
+        idx = g.lir + q - 1 - S.ibase;
+        return false;
+    }
     if (x < g.l + g.i) {
         uint64_t j, t;
         S.fd.divmod(x, j, t);
@@ -95,6 +145,41 @@ TL_HD bool btree_place(const BtreeStream &S, uint64_t x, uint64_t &idx) {
     return false;
 }
 
+// Final position of the key held by scratch slot `slot`.
+TL_HD uint64_t btree_slot_dest(const BtreeStream &S, uint64_t slot) {
+    const BtreeGeom &g = S.g;
+    if (S.plan == PLAN_R) return btree_perfect_pos(g, S.fd, slot, g.h);
+    uint64_t s;
+    if (slot < g.lir) {
+        s = slot;
+    } else {
+        const uint64_t M = slot - g.lir + S.ibase + 1;
+        s = M * (g.b + 1) - 1 + g.l + g.r;
+    }
+    return btree_pos(g, S.fd, s);
+}
+
+__host__ inline void btree_choose_plan(BtreeStream &S) {
+    const BtreeGeom &g = S.g;
+    S.plan = PLAN_R;
+    S.nscratch = g.ni;
+    if (g.h < 1) return;
+    const uint64_t i2 = g.pw[g.h - 1] - 1;
+    const uint64_t ibase = g.i / (g.b + 1);
+    // Plan L needs every direct key to move left: i2 <= l + r + floor((c+1)/(b+1))
+    // at the smallest trailing top rank c = i.
+    if (g.lir >= g.n) return;
+    if (i2 > g.l + g.r + (g.i + 1) / (g.b + 1)) return;
+    const uint64_t upper = g.ni / (g.b + 1) - ibase;
+    const uint64_t nscr = g.lir + upper;
+    if (nscr < g.ni) {
+        S.plan = PLAN_L;
+        S.i2 = i2;
+        S.ibase = ibase;
+        S.nscratch = nscr;
+    }
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kStreamThreads)
 btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl *ctrl, unsigned int *flags) {
@@ -105,7 +190,7 @@ btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl 
     for (;;) {
         unsigned long long t = next_ticket(ctrl, &s_ticket);
         if (t >= S.ntiles) break;
-        const uint64_t k = S.ntiles - 1 - t;  // right to left
+        const uint64_t k = btree_tile_of_ticket(S, t);
         uint64_t p0, p1;
         btree_tile(S, k, p0, p1);
         const uint64_t base = load_tile(A, p0, p1, sm);
@@ -125,13 +210,12 @@ btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl 
     }
 }
 
-// Scratch holds the top tree in sorted order (top rank c at scr[c]).
 template <typename K>
 __global__ void __launch_bounds__(kScatterThreads)
-btree_scatter_top_kernel(K *__restrict__ A, const K *__restrict__ scr, BtreeStream S) {
+btree_scatter_kernel(K *__restrict__ A, const K *__restrict__ scr, BtreeStream S) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < S.g.ni; c += stride)
-        A[btree_perfect_pos(S.g, S.fd, c, S.g.h)] = __ldcs(scr + c);
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < S.nscratch; c += stride)
+        A[btree_slot_dest(S, c)] = __ldcs(scr + c);
 }
 
 // ---------------------------------------------------------------- mvEB stream
@@ -299,7 +383,8 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
         pl.bs.tile_keys = pl.tile_keys;
         pl.ntiles = (n + pl.tile_keys - 1) / pl.tile_keys;
         pl.bs.ntiles = pl.ntiles;
-        pl.scratch_keys = pl.bs.g.ni;
+        btree_choose_plan(pl.bs);
+        pl.scratch_keys = pl.bs.nscratch;
     }
     pl.off_flags = align_up(pl.scratch_keys * key_bytes, 256);
     pl.off_ctrl = pl.off_flags + align_up(pl.ntiles * sizeof(unsigned int), 256);
@@ -360,7 +445,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         if (pl.scratch_keys) {
             uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterThreads - 1) / kScatterThreads,
                                              (uint64_t)smx * 8);
-            btree_scatter_top_kernel<K><<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.bs);
+            btree_scatter_kernel<K><<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.bs);
             TL_CUDA_TRY(cudaGetLastError());
         }
     }
@@ -381,6 +466,12 @@ static void keep_pool_memory() {
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     });
+}
+
+int btree_plan_of(uint64_t n, uint64_t b) {
+    PermutePlan pl;
+    if (make_plan(TL_LAYOUT_BTREE, n, b, 8, pl)) return -1;
+    return pl.bs.plan;
 }
 
 int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes) {
@@ -452,7 +543,7 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
         const MvebPlan &P = pl.mp.plan;
         auto tile_of = [&](uint64_t d) { return mv ? mveb_tile_of(P, d) : d / pl.tile_keys; };
         for (uint64_t t = 0; t < pl.ntiles; ++t) {
-            const uint64_t k = pl.ntiles - 1 - t;
+            const uint64_t k = mv ? pl.ntiles - 1 - t : btree_tile_of_ticket(pl.bs, t);
             uint64_t p0, p1, k_lo = 0, k_hi = 0;
             int ri = 0;
             if (mv) mveb_tile(P, k, ri, p0, p1); else btree_tile(pl.bs, k, p0, p1);
@@ -464,8 +555,10 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
             const bool wait = mv ? mveb_tile_wait(P, P.reg[ri], p0, p1, k_lo, k_hi)
                                  : btree_tile_wait(pl.bs, p0, p1, k_lo, k_hi);
             if (wait)
-                for (uint64_t kk = k_lo; kk <= k_hi; ++kk)
-                    if (kk <= k || !readk[kk]) ++viol;
+                for (uint64_t kk = k_lo; kk <= k_hi; ++kk) {
+                    const bool earlier = (mv || pl.bs.plan == PLAN_R) ? kk > k : kk < k;
+                    if (!earlier || !readk[kk]) ++viol;
+                }
             auto W = [&](uint64_t d, uint64_t v) {
                 if (d >= n) { ++viol; return; }
                 const uint64_t kd = tile_of(d);
@@ -508,9 +601,10 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
             }
         }
         if (!mv) {
-            for (uint64_t c = 0; c < pl.bs.g.ni; ++c) {
+            for (uint64_t c = 0; c < pl.bs.nscratch; ++c) {
                 if (slot_writes[c] != 1) ++viol;
-                const uint64_t d = btree_perfect_pos(pl.bs.g, pl.bs.fd, c, pl.bs.g.h);
+                const uint64_t d = btree_slot_dest(pl.bs, c);
+                if (d >= n) { ++viol; continue; }
                 A[d] = scr[c];
                 ++pos_writes[d];
             }
