@@ -94,6 +94,20 @@ int tl_permute_btree_u64(uint64_t *dev_A, uint64_t n, uint64_t b, void *stream, 
 int tl_permute_mveb_u32(uint32_t *dev_A, uint64_t n, void *stream, float *ms);
 int tl_permute_mveb_u64(uint64_t *dev_A, uint64_t n, void *stream, float *ms);
 
+/* No counterpart in the reference.  tl_permute for callers that cannot allocate
+ * device memory (a plugin inside a host engine that owns every allocation, a
+ * latency-bound service that must not hit cudaMalloc's implicit synchronisation
+ * mid-request): the workspace is a fixed array of TL_STATIC_WORKSPACE_BYTES
+ * compiled into the library, present on every GPU that loads it until the
+ * process exits.  Permutations whose tl_permute_workspace_bytes exceeds it
+ * return TL_ERROR_UNSUPPORTED.  All calls share that array: calls that overlap
+ * on the GPU race, so serialise them.  The first call on a device looks the
+ * array up (cudaGetSymbolAddress); make it before any stream capture.
+ * Synchronous like tl_permute; allocates nothing. */
+#define TL_STATIC_WORKSPACE_BYTES (32ull << 20)
+int tl_permute_static_ws(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
+                         void *stream);
+
 /* ---------------------------------------------------------------- mvEB tables */
 /* buildTable(vEB_table *table, uint64_t n, uint32_t d, uint32_t root_depth):
  * gpu/src/query-mveb.cu:25-47.  Host function; table holds d entries, zeroed by
