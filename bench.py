@@ -24,7 +24,6 @@ import ctypes as C
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -86,50 +85,54 @@ def reduce_max(x, world):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled through NVML every few ms while the
+    timed region runs (same counters as nvidia-smi's clocks/clocks_event_reasons)."""
+    REASONS = {  # NVML clocks-event-reason bits
+        "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+        "hw_power_brake_slowdown": 0x80, "sw_power_cap": 0x4,
+    }
 
-    def __init__(self, index):
-        self.index = index
-        self.p = None
-        self.path = os.path.join("/tmp", f"tl_clocks_{os.getpid()}.csv")
+    def __init__(self, index, period_s=0.005):
+        self.index, self.period = index, period_s
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.ok = True
+        except Exception as e:  # no NVML: report it rather than invent numbers
+            self.err = repr(e)
+
+    def _run(self):
+        while not self.stop_evt.is_set():
+            try:
+                self.samples.append(float(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)))
+                bits = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if bits & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self.stop_evt.wait(self.period)
 
     def start(self):
-        try:
-            self.f = open(self.path, "w")
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
+        import threading
+        if not self.ok:
+            return
+        self.stop_evt = threading.Event()
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
 
     def stop(self):
-        if self.p is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        self.f.close()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"nvml unavailable: {self.err}"]}
+        self.stop_evt.set()
+        self.t.join()
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 def cpu_reference_permute(layout, b, n_sample, key_bytes, reps, min_seconds=8.0):
@@ -193,6 +196,130 @@ def run_reference(args, rank):
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def learned_section(args, dev):
+    """Learned-start vs plain B-tree queries on skewed keys: n = 2^30 unique
+    uint64 keys (lognormal + clusters, seed 8), b = 16, q = 2^28 queries (seed 9,
+    90% Zipf(1.1) hits, 10% uniform misses).  The model is trained on the sorted
+    keys by the library's own kernels, then the keys are permuted in place."""
+    import numpy as np
+    import torch
+
+    import tree_layouts as T
+    import tree_layouts.learned as LL
+    from tree_layouts import data
+
+    n, b, q = args.learned_n, 16, args.learned_q
+    t0 = time.time()
+    keys = data.skewed_keys_torch(n, 8, dev)
+    gen_s = time.time() - t0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    model, leaves = LL.train(keys, num_leaves=65536, steps=args.learned_steps, batch=65536, lr=3e-3, seed=1)
+    ev1.record()
+    torch.cuda.synchronize()
+    train_ms = ev0.elapsed_time(ev1)
+    Q = data.zipf_queries_torch(keys, q, 9)
+    T.permute("btree", keys, b)  # keys now hold the layout
+    tree = keys
+    plain = torch.empty(q, dtype=torch.int64, device=dev)
+    learned = torch.empty_like(plain)
+    stats = torch.zeros(2, dtype=torch.int64, device=dev)
+    for _ in range(2):
+        T.query("btree", tree, Q, plain, b)
+        LL.query(tree, model, leaves, Q, learned, b)
+    p_ms, l_ms = [], []
+    for _ in range(3):
+        p_ms.append(T.query("btree", tree, Q, plain, b, timed=True))
+        l_ms.append(LL.query(tree, model, leaves, Q, learned, b, timed=True))
+    LL.query(tree, model, leaves, Q, learned, b, stats=stats)
+    exact = bool(torch.equal(plain, learned))
+    lv = LL.leaves_numpy(leaves)
+    used = lv["empty"] == 0
+    win = (lv["eps_lo"].astype(np.int64) + lv["eps_hi"])[used]
+    pm, lm = statistics.median(p_ms), statistics.median(l_ms)
+    out = {"workload": "btree-b16-n2^30-u64 skewed keys (lognormal sigma=2 + 5% in 1000 clusters), "
+                       "2^28 queries 90% Zipf(1.1) / 10% uniform misses",
+           "n": n, "q": q, "plain_queries_per_s": round(q / (pm * 1e-3), 1),
+           "learned_queries_per_s": round(q / (lm * 1e-3), 1), "speedup": round(pm / lm, 3),
+           "exact": exact, "plain_ms": round(pm, 3), "learned_ms": round(lm, 3),
+           "fallback_frac": round(int(stats[0].item()) / q, 4),
+           "mean_start_depth": round(int(stats[1].item()) / q, 3),
+           "train_ms": round(train_ms, 1), "train_loss": model.train_loss, "keygen_s": round(gen_s, 1),
+           "leaves_used": int(used.sum()), "window_median": int(np.median(win)),
+           "window_p99": int(np.percentile(win, 99))}
+    del keys, tree, Q, plain, learned, leaves
+    torch.cuda.empty_cache()
+    return out
+
+
+def batched_section(args, dev):
+    """Batched permute + queries: 4096 sorted uint64 arrays, sizes log-uniform in
+    [2^10, 2^22] (seed 7), keys prefix sums of uniform gaps in [1, 64], int64
+    offsets; each permuted to a B-tree with b = 8 by one persistent launch
+    replayed from a CUDA graph; 2^26 queries with uniform instance ids, 70% hits.
+    The autotuner picks the tuning first (on the same data, left sorted)."""
+    import torch
+
+    import tree_layouts as T
+    import tree_layouts.batched as TB
+    from tree_layouts import data
+
+    sizes = TB.batch_sizes_np(args.batch_num, 10, 22, 7)
+    keys, off = data.batch_keys_torch(sizes, 64, 7, dev)
+    total = int(sizes.sum())
+    Q, inst = data.batch_queries_torch(keys, off, args.batch_q, 0.7, 8)
+    plan = TB.BatchPlan(off, b=8)
+    t0 = time.time()
+    report = plan.autotune(keys, Q, inst)
+    tune_s = time.time() - t0
+    pristine = keys.clone()
+    ws = plan.workspace()
+    s = torch.cuda.Stream()
+    plan.permute(keys, ws, stream=s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        plan.permute(keys, ws, stream=s, check=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for i in range(args.warmup + args.steps):
+        keys.copy_(pristine)
+        torch.cuda.synchronize()
+        e0.record(s)
+        g.replay()
+        e1.record(s)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    plan.status(ws)
+    # exactness spot check: instances against the single-array entry point
+    offs = off.cpu().numpy()
+    rng = __import__("numpy").random.default_rng(1)
+    checked = 0
+    for j in rng.integers(0, len(sizes), 24):
+        a = pristine[offs[j]:offs[j + 1]].clone()
+        T.permute("btree", a, 8)
+        assert torch.equal(a, keys[offs[j]:offs[j + 1]]), f"instance {j} differs"
+        checked += 1
+    ans = torch.empty(Q.numel(), dtype=torch.int64, device=dev)
+    for _ in range(2):
+        plan.query(keys, Q, inst, ans)
+    qms = statistics.median(plan.query(keys, Q, inst, ans, timed=True) for _ in range(3))
+    del g
+    pm = statistics.median(ms)
+    out = {"workload": "4096 uint64 arrays, sizes log-uniform [2^10, 2^22], b = 8, one persistent launch "
+                       "replayed from a CUDA graph; 2^26 queries, 70% hits",
+           "arrays": len(sizes), "total_keys": total,
+           "permute_ms": round(pm, 3), "permute_GBps": round(2.0 * total * 8 / (pm * 1e-3) / 1e9, 1),
+           "permute_frac_of_peak": round(2.0 * total * 8 / (pm * 1e-3) / 1e9 / peaks()[0], 4),
+           "queries": Q.numel(), "query_ms": round(qms, 3), "queries_per_s": round(Q.numel() / (qms * 1e-3), 1),
+           "autotune_s": round(tune_s, 2), "tuning": {k: report[k] for k in ("threads", "query_chunk")},
+           "instances_checked": checked}
+    del keys, pristine, Q, inst, ans, ws
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args, rank, world, local):
@@ -300,6 +427,16 @@ def run_ours(args, rank, world, local):
                "h2d_bytes_per_step": n * kb, "d2h_bytes_per_step": n * kb, "ms_per_step": round(ems, 3)}
         del host_in, host_out
 
+    lrn = None
+    del A, pristine
+    torch.cuda.empty_cache()
+    if args.learned and layout == "btree" and rank == 0:
+        lrn = learned_section(args, dev)
+
+    bat = None
+    if args.batched and layout == "btree" and rank == 0:
+        bat = batched_section(args, dev)
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample > 0 and layout != "mveb":
         cpu = cpu_reference_permute(layout, b, min(n, args.cpu_sample), kb, 5)
@@ -324,6 +461,8 @@ def run_ours(args, rank, world, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "queries": qinfo,
+            "learned": lrn,
+            "batched": bat,
             "clocks": clk,
             "gpu_launches": 2 * args.steps,
         }
@@ -341,6 +480,13 @@ def main():
     ap.add_argument("--queries", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=50_000_000)
+    ap.add_argument("--learned", type=int, default=1, help="learned-vs-plain query section (B-tree workloads)")
+    ap.add_argument("--learned-n", type=int, default=2**30)
+    ap.add_argument("--learned-q", type=int, default=2**28)
+    ap.add_argument("--learned-steps", type=int, default=1500)
+    ap.add_argument("--batched", type=int, default=1, help="batched permute/query section (B-tree workloads)")
+    ap.add_argument("--batch-num", type=int, default=4096)
+    ap.add_argument("--batch-q", type=int, default=2**26)
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

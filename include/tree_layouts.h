@@ -156,6 +156,112 @@ int tl_query_veb_nonperfect_u64(const uint64_t *dev_layout, const tl_veb_table *
                                 const uint64_t *dev_queries, uint64_t q, uint64_t *dev_answers,
                                 void *stream, float *ms);
 
+/* ---------------------------------------------------------------- batched mode
+ * No counterpart in the reference.  num independent sorted arrays of uneven
+ * sizes, concatenated in one device buffer and described by an int64 offset
+ * table (offsets[num] = total keys), each permuted to a level-order B-tree of b
+ * keys per node (tl_permute's layout, per instance) by one persistent kernel,
+ * and queried by a batch of (key, instance) pairs. */
+typedef struct tl_batch_plan tl_batch_plan;
+/* Builds the per-instance schedules on the device from dev_offsets (num + 1
+ * entries) and sizes the workspace (synchronises the stream once). */
+int tl_batch_plan_create(const int64_t *dev_offsets, uint32_t num, uint64_t b, uint32_t key_bytes,
+                         void *stream, tl_batch_plan **plan);
+int tl_batch_plan_destroy(tl_batch_plan *plan);
+int tl_batch_workspace_bytes(const tl_batch_plan *plan, uint64_t *bytes);
+/* Permutes every instance in place: one memset and one persistent kernel on
+ * `stream`, no host synchronisation, capturable in a CUDA graph.  The status of
+ * its bounded waits is read by tl_batch_status. */
+int tl_batch_permute(const tl_batch_plan *plan, void *dev_keys, void *dev_workspace, uint64_t workspace_bytes,
+                     void *stream);
+int tl_batch_status(const tl_batch_plan *plan, const void *dev_workspace, void *stream);
+int tl_batch_query_workspace_bytes(const tl_batch_plan *plan, uint64_t q, uint64_t *bytes);
+/* dev_answers[i] = position of dev_queries[i] inside instance dev_inst[i]'s
+ * layout (0-based within the instance), or that instance's n when absent; 0 for
+ * an instance id >= num. */
+int tl_batch_query(const tl_batch_plan *plan, const void *dev_keys, const void *dev_queries,
+                   const uint32_t *dev_inst, uint64_t q, uint64_t *dev_answers, void *dev_workspace,
+                   uint64_t workspace_bytes, void *stream, float *ms);
+/* Tuning per size class c = floor(log2 n_j), 48 entries each: keys per stream
+ * tile, top levels pinned in shared memory by the query; plus the query work
+ * item and the permute block size (256 or 512); 0 / NULL keeps a value.
+ * Changing tile sizes rebuilds the plan from dev_offsets. */
+int tl_batch_set_tuning(tl_batch_plan *plan, const uint32_t *tile_keys, const uint32_t *pin_levels,
+                        uint32_t query_chunk, uint32_t threads, const int64_t *dev_offsets, void *stream);
+int tl_batch_get_tuning(const tl_batch_plan *plan, uint32_t *tile_keys, uint32_t *pin_levels,
+                        uint32_t *query_chunk, uint32_t *threads);
+/* Measures and keeps the best tuning (coordinate descent over the block size,
+ * per-class tile sizes, the query work item and per-class pinned levels) on the
+ * caller's data; dev_keys must hold the sorted instances and is left sorted.
+ * report (optional) receives a JSON summary. */
+int tl_batch_autotune(tl_batch_plan *plan, const int64_t *dev_offsets, void *dev_keys, const void *dev_queries,
+                      const uint32_t *dev_inst, uint64_t q, void *stream, char *report, uint64_t report_len);
+
+/* ---------------------------------------------------------------- learned-start B-tree query
+ * No counterpart in the reference.  A two-stage rank model over the sorted keys:
+ * an FP32 root MLP 1 -> 32 -> 32 -> 1 over the normalised key (linear or log2
+ * scale) picks one of num_leaves linear segments; a segment predicts the rank
+ * and records its largest rank errors below and above the prediction over the
+ * keys it was fitted on.  The learned query starts its descent at the deepest
+ * subtree whose rank range covers [rank - eps_lo, rank + eps_hi] and falls back to
+ * the full search whenever that start cannot decide, so answers equal
+ * tl_query_btree_u64's. */
+#define TL_RMI_HIDDEN 32
+typedef struct tl_rank_model {
+    float w1[TL_RMI_HIDDEN], b1[TL_RMI_HIDDEN];                    /* 1 -> 32, ReLU */
+    float w2[TL_RMI_HIDDEN][TL_RMI_HIDDEN], b2[TL_RMI_HIDDEN];     /* 32 -> 32, ReLU; w2[out][in] */
+    float w3[TL_RMI_HIDDEN], b3;                                   /* 32 -> 1: rank / n */
+    float train_loss;                                              /* last training batch's MSE */
+    double x_lo, x_scale;          /* x = clamp((f(key) - x_lo) * x_scale, 0, 1) */
+    uint64_t n;                    /* number of keys the model was fitted on */
+    uint32_t log_feature;          /* f(key) = log2(key + 1) if set, else key */
+    uint32_t num_leaves;           /* power of two */
+    uint32_t train_root;           /* 0: root network replaced by the identity (ablation) */
+    uint32_t reserved;
+} tl_rank_model;
+
+typedef struct tl_rank_leaf {
+    uint64_t kmin;     /* smallest key of the segment */
+    uint64_t base;     /* its rank */
+    float slope;       /* ranks per key unit */
+    uint32_t eps_lo;   /* largest (prediction - rank) over the segment's keys */
+    uint32_t eps_hi;   /* largest (rank - prediction) over the segment's keys */
+    uint32_t empty;    /* 1: no key maps to this segment */
+} tl_rank_leaf;
+
+typedef struct tl_rank_train_config {
+    uint32_t num_leaves;   /* e.g. 65536 */
+    uint32_t steps;        /* Adam steps on the root network */
+    uint32_t batch;        /* (key, rank) samples per step */
+    uint32_t log_feature;
+    uint32_t train_root;   /* 0 = leaf-only ablation */
+    uint32_t monotone;     /* 1: keep w1, w2, w3 >= 0 (the root is then non-decreasing in the key) */
+    float lr;              /* Adam step size */
+    uint64_t seed;
+} tl_rank_train_config;
+
+/* Trains the root network on (key, rank) pairs of the sorted keys (hand-written
+ * forward/backward/Adam kernels), fits num_leaves segments and their eps.
+ * dev_leaves holds num_leaves entries. */
+int tl_rank_model_train(const uint64_t *dev_sorted_keys, uint64_t n, const tl_rank_train_config *cfg,
+                        tl_rank_model *model, tl_rank_leaf *dev_leaves, void *stream);
+/* Inference: dev_rank[i] = predicted rank of dev_keys[i]; dev_eps[i] (optional) =
+ * max(eps_lo, eps_hi) of its segment (UINT32_MAX for an empty segment). */
+int tl_rank_model_predict(const tl_rank_model *model, const tl_rank_leaf *dev_leaves,
+                          const uint64_t *dev_keys, uint64_t q, uint64_t *dev_rank, uint32_t *dev_eps,
+                          void *stream);
+/* Gradient of the mean squared error of the root network on (x, y) samples
+ * (dev_x normalised features, dev_y = rank / n), as computed by the training
+ * kernels: host_grad[1153] in the order w1, b1, w2, b2, w3, b3. */
+int tl_rank_model_gradient(const tl_rank_model *model, const float *dev_x, const float *dev_y, uint32_t m,
+                           float *host_grad, float *host_loss, void *stream);
+/* Learned-start query over a B-tree layout of the model's n keys (b*8 a multiple
+ * of 16, b <= 32).  dev_stats (optional, 2 words, accumulated): number of
+ * queries that fell back to the full search, sum of start depths. */
+int tl_query_btree_learned_u64(const uint64_t *dev_layout, uint64_t n, uint64_t b, const tl_rank_model *model,
+                               const tl_rank_leaf *dev_leaves, const uint64_t *dev_queries, uint64_t q,
+                               uint64_t *dev_answers, unsigned long long *dev_stats, void *stream, float *ms);
+
 /* ---------------------------------------------------------------- test and profiling hooks */
 /* Bound every device-side wait to spin_limit iterations (0 = default, about one
  * second) and, when force_timeout != 0, make the waits expect a flag value no
@@ -166,6 +272,9 @@ int tl_debug_set_wait(unsigned int spin_limit, int force_timeout);
  * protocol breaches (stale read, unguarded store, bad wait, position or scratch
  * slot not written exactly once). */
 int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations);
+/* sizeof of the ABI structs, for bindings to check their mirrors:
+ * 0 tl_veb_table, 1 tl_rank_model, 2 tl_rank_leaf, 3 tl_rank_train_config. */
+int tl_debug_struct_size(int which);
 /* Schedule the B-tree permutation uses for (n, b): 0 right-to-left, 1 left-to-right. */
 int tl_debug_btree_plan(uint64_t n, uint64_t b);
 /* tl_permute with library-allocated workspace, reporting the device time of its

@@ -1,0 +1,98 @@
+"""Learned-start B-tree query: hand-written training kernels checked against the
+float64 CPU oracle, exact answers (identical to the plain B-tree query for every
+query), and what the trained root network gains over the same method without
+it (leaf segments indexed by the normalised key directly)."""
+import numpy as np
+import pytest
+
+import rank_model as R
+import tree_layouts as T
+import tree_layouts.learned as LL
+from tree_layouts import data
+
+pytestmark = pytest.mark.gpu
+
+
+def _keys(n, seed=8):
+    return data.skewed_keys_torch(n, seed)
+
+
+def test_gradient_matches_cpu_double_oracle():
+    import torch
+    keys = _keys(1 << 16)
+    model, _ = LL.train(keys, num_leaves=1024, steps=0, train_root=True)  # initial weights only
+    rng = np.random.default_rng(3)
+    for m in (64, 1000, 4096):
+        x = rng.random(m).astype(np.float32)
+        y = np.clip(x ** 0.5 + rng.normal(0, 0.01, m), 0, 1).astype(np.float32)
+        g_gpu, loss_gpu = LL.gradient(model, torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda())
+        loss_ref, g_ref = R.loss_and_grad(model.flat(), x.astype(np.float64), y.astype(np.float64))
+        assert abs(loss_gpu - loss_ref) <= 1e-5 + 1e-4 * abs(loss_ref)
+        # float32 kernels vs float64: relative to the gradient's scale
+        scale = np.abs(g_ref).max()
+        assert np.abs(g_gpu - g_ref).max() <= 2e-4 * scale, (m, np.abs(g_gpu - g_ref).max(), scale)
+
+
+def test_training_fits_the_rank_function():
+    keys = _keys(1 << 22)
+    model, leaves = LL.train(keys, num_leaves=4096, steps=600, batch=16384)
+    lv = LL.leaves_numpy(leaves)
+    used = lv["empty"] == 0
+    assert model.train_loss < 1e-3
+    assert used.mean() > 0.5  # the root spreads keys over the segments
+    # eps is the real maximum error: check with the inference kernel
+    rank, eps = LL.predict(model, leaves, keys)
+    import torch
+    truth = torch.arange(keys.numel(), device="cuda")
+    err = (rank - truth).abs()
+    assert bool((err <= eps.to(torch.int64) & 0xFFFFFFFF).all())
+
+
+@pytest.mark.parametrize("n,b", [(1 << 22, 16), (3_000_017, 16), (2_000_000, 8), (1_048_575, 4)])
+def test_learned_answers_equal_plain_answers(n, b):
+    import torch
+    keys = _keys(n, seed=n % 97)
+    model, leaves = LL.train(keys, num_leaves=1 << 12, steps=300, batch=16384)
+    tree = keys.clone()
+    T.permute("btree", tree, b)
+    Q = torch.cat([data.zipf_queries_torch(keys, 200_000, 5), keys[:1000] + 1, keys[-5:],
+                   torch.tensor([0, 1, 2**62, 2**62 + 5], device="cuda")])
+    plain = torch.empty(Q.numel(), dtype=torch.int64, device="cuda")
+    learned = torch.empty_like(plain)
+    stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+    T.query("btree", tree, Q, plain, b)
+    LL.query(tree, model, leaves, Q, learned, b, stats=stats)
+    assert torch.equal(plain, learned)
+    hit = plain != n
+    assert torch.equal(tree[plain[hit]], Q[hit])
+
+
+def test_trained_network_beats_leaf_only_method():
+    """What the trained root network gains over the same two-stage method
+    without it (segments indexed by the normalised key directly): per query,
+    fewer full-search fallbacks and a narrower rank window (so a deeper start);
+    and the learned start beats the plain full-depth search."""
+    import torch
+    n, b = 1 << 24, 16
+    keys = _keys(n, seed=8)
+    tree = keys.clone()
+    T.permute("btree", tree, b)
+    Q = data.zipf_queries_torch(keys, 1 << 22, 9)
+    out = torch.empty(Q.numel(), dtype=torch.int64, device="cuda")
+    plain_ms = min(T.query("btree", tree, Q, out, b, timed=True) for _ in range(3))
+    ref = out.clone()
+    res = {}
+    for trained in (True, False):
+        model, leaves = LL.train(keys, num_leaves=1 << 16, steps=800, batch=65536, train_root=trained)
+        _, eps = LL.predict(model, leaves, keys)  # each key's segment eps
+        win = torch.log2(2.0 * (eps.to(torch.int64) & 0xFFFFFFFF).double() + 1.0).mean().item()
+        stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+        LL.query(tree, model, leaves, Q, out, b, stats=stats)
+        assert torch.equal(out, ref)
+        ms = min(LL.query(tree, model, leaves, Q, out, b, timed=True) for _ in range(3))
+        res[trained] = {"key_log_window": win, "fallback": int(stats[0].item()) / Q.numel(),
+                        "start_depth": int(stats[1].item()) / Q.numel(), "ms": ms}
+    print("ablation", res, "plain_ms", plain_ms)
+    assert res[True]["fallback"] < res[False]["fallback"], res
+    assert res[True]["key_log_window"] < res[False]["key_log_window"], res
+    assert res[True]["ms"] < plain_ms, (res, plain_ms)

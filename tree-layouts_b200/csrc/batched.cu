@@ -1,0 +1,703 @@
+// Batched mode (no counterpart in the reference): many independent sorted
+// arrays of uneven sizes, concatenated and described by an int64 offset table,
+// are each permuted into a B-tree layout by ONE persistent kernel launch, and
+// queried by one batch of (key, instance) pairs.
+//
+// Plan (built once per offset table, on the device): a setup kernel computes
+// every instance's geometry and schedule (the same host/device helpers as the
+// single-array path), its tile count, scratch size and scatter-chunk count, and
+// exclusive prefix sums of them.  Execute: a memset of the control words and one
+// persistent kernel; tickets 0..T-1 are stream tiles (instance by instance, each
+// in its own plan's direction), tickets T.. are scatter chunks.  A chunk of
+// instance j starts once all of j's tiles have stored (a per-instance counter,
+// bounded wait); stream tiles never wait on chunks, so every wait ends.
+// Per size class (floor(log2 n_j)) the tile size comes from a tuning table that
+// tl_batch_autotune fills by measurement.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "batched.h"
+#include "btree_plan.cuh"
+#include "internal.h"
+
+namespace tl {
+
+constexpr int kBatchThreads = 256;     // query kernel
+constexpr int kBatchMaxThreads = 512;  // permute kernel: 256 or 512 (tuned)
+constexpr int kMaxClass = 48;
+
+struct BatchInst {
+    BtreeStream S;
+    uint64_t off;          // first key of the instance
+    uint64_t tile_base;    // first global tile
+    uint64_t scr_base;     // first scratch slot
+    uint64_t chunk_base;   // first global scatter chunk
+    uint64_t nchunks;
+};
+
+struct BatchTotals {
+    uint64_t tiles, chunks, scratch, max_tile;
+};
+
+struct tl_batch_plan_impl {
+    uint32_t num = 0, key_bytes = 8;
+    uint64_t b = 8;
+    BatchInst *inst = nullptr;   // device
+    BatchTotals tot{};
+    uint32_t tile_keys[kMaxClass];
+    uint32_t pin_levels[kMaxClass];  // query: top levels pinned in shared memory per size class
+    uint32_t query_chunk = 2048;     // queries per CTA work item
+    uint32_t threads = 256;          // permute kernel block size
+    uint64_t off_flags = 0, off_done = 0, off_ctrl = 0, ws_bytes = 0;
+    uint64_t total_keys = 0;
+};
+
+// ---------------------------------------------------------------- setup
+__global__ void __launch_bounds__(256) batch_setup_kernel(const int64_t *__restrict__ offsets, uint32_t num, uint64_t b, FastDiv64 fd,
+                                   FastDiv32 fd32, const uint32_t *__restrict__ tile_keys,
+                                   BatchInst *__restrict__ inst, BatchTotals *__restrict__ tot) {
+    // one block: per-instance plans, then exclusive scans in instance order
+    __shared__ unsigned long long s_part[3][1024];
+    const uint32_t T = blockDim.x;
+    const uint32_t per = (num + T - 1) / T;
+    const uint32_t j0 = threadIdx.x * per, j1 = min(num, j0 + per);
+    unsigned long long st = 0, ss = 0, sc = 0;
+    for (uint32_t j = j0; j < j1; ++j) {
+        BatchInst I;
+        memset(&I, 0, sizeof I);
+        const uint64_t n = (uint64_t)(offsets[j + 1] - offsets[j]);
+        I.off = (uint64_t)offsets[j];
+        I.S.g = make_btree_geom(n, b);
+        I.S.fd = fd;
+        I.S.fd32 = fd32;
+        const uint32_t cls = n ? bit_length(n) - 1 : 0;
+        I.S.tile_keys = tile_keys[cls < kMaxClass ? cls : kMaxClass - 1];
+        I.S.ntiles = (n + I.S.tile_keys - 1) / I.S.tile_keys;
+        btree_choose_plan(I.S);
+        if (n <= 1) {
+            I.S.ntiles = 0;
+            I.S.nscratch = 0;
+        }
+        I.nchunks = (I.S.nscratch + kScatterChunk - 1) / kScatterChunk;
+        st += I.S.ntiles;
+        ss += I.S.nscratch;
+        sc += I.nchunks;
+        inst[j] = I;
+    }
+    s_part[0][threadIdx.x] = st;
+    s_part[1][threadIdx.x] = ss;
+    s_part[2][threadIdx.x] = sc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long a = 0, c = 0, d = 0;
+        for (uint32_t t = 0; t < T; ++t) {
+            const unsigned long long x = s_part[0][t], y = s_part[1][t], z = s_part[2][t];
+            s_part[0][t] = a;
+            s_part[1][t] = c;
+            s_part[2][t] = d;
+            a += x;
+            c += y;
+            d += z;
+        }
+        tot->tiles = a;
+        tot->scratch = c;
+        tot->chunks = d;
+        uint64_t mt = 0;
+        for (int k = 0; k < kMaxClass; ++k) mt = max(mt, (uint64_t)tile_keys[k]);
+        tot->max_tile = mt;
+    }
+    __syncthreads();
+    unsigned long long bt = s_part[0][threadIdx.x], bs = s_part[1][threadIdx.x], bc = s_part[2][threadIdx.x];
+    for (uint32_t j = j0; j < j1; ++j) {
+        inst[j].tile_base = bt;
+        inst[j].scr_base = bs;
+        inst[j].chunk_base = bc;
+        bt += inst[j].S.ntiles;
+        bs += inst[j].S.nscratch;
+        bc += inst[j].nchunks;
+    }
+}
+
+// Last instance j with field(j) <= x (fields ascend with j).
+template <typename F>
+__device__ __forceinline__ uint32_t find_inst(const BatchInst *inst, uint32_t num, uint64_t x, F field) {
+    uint32_t lo = 0, hi = num - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (field(inst[mid]) <= x) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------- permute
+template <typename K>
+__global__ void __launch_bounds__(kBatchMaxThreads, 1)
+batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst *__restrict__ inst, uint32_t num,
+                     BatchTotals tot, Ctrl *ctrl, WaitCfg wc, unsigned int *flags, unsigned int *done) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *sm = reinterpret_cast<K *>(smem_raw);
+    __shared__ unsigned long long s_ticket;
+    __shared__ int s_ok;
+    __shared__ uint32_t s_j;
+    for (;;) {
+        const unsigned long long t = next_ticket(ctrl, &s_ticket);
+        if (t >= tot.tiles + tot.chunks) break;
+        if (t < tot.tiles) {
+            if (threadIdx.x == 0) s_j = find_inst(inst, num, t, [](const BatchInst &I) { return I.tile_base; });
+            __syncthreads();
+            const BatchInst &I = inst[s_j];
+            const uint64_t k = btree_tile_of_ticket(I.S, t - I.tile_base);
+            btree_stream_tile(I.S, keys + I.off, scr + I.scr_base, flags + I.tile_base, ctrl, wc, k, sm, &s_ok);
+            __syncthreads();  // every store of the tile issued before it counts as done
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicAdd(&done[s_j], 1u);
+            }
+        } else {
+            const uint64_t c = t - tot.tiles;
+            if (threadIdx.x == 0) {
+                s_j = find_inst(inst, num, c, [](const BatchInst &I) { return I.chunk_base; });
+                const unsigned int need = (unsigned int)inst[s_j].S.ntiles;
+                s_ok = wait_flag(&done[s_j], need, ctrl, wc) ? 1 : 0;
+            }
+            __syncthreads();
+            if (!s_ok) continue;
+            const BatchInst &I = inst[s_j];
+            btree_scatter_chunk(I.S, keys + I.off, scr + I.scr_base, (c - I.chunk_base) * kScatterChunk);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- queries
+// Queries are grouped by instance (counting sort: histogram, scan, scatter) so
+// that a CTA's work item mostly belongs to one instance; the CTA then pins that
+// instance's top levels in shared memory (depth from the size-class table).
+__global__ void batch_hist_kernel(const uint32_t *__restrict__ qinst, uint64_t q, uint32_t num,
+                                  unsigned int *__restrict__ count) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < q; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = qinst[i];
+        if (j < num) atomicAdd(&count[j], 1u);
+    }
+}
+
+__global__ void batch_scan_kernel(const unsigned int *__restrict__ count, uint32_t num,
+                                  unsigned long long *__restrict__ start) {
+    __shared__ unsigned long long s_part[1024];
+    const uint32_t T = blockDim.x, per = (num + T - 1) / T;
+    const uint32_t j0 = threadIdx.x * per, j1 = min(num, j0 + per);
+    unsigned long long acc = 0;
+    for (uint32_t j = j0; j < j1; ++j) acc += count[j];
+    s_part[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long a = 0;
+        for (uint32_t t = 0; t < T; ++t) {
+            const unsigned long long x = s_part[t];
+            s_part[t] = a;
+            a += x;
+        }
+        start[num] = a;
+    }
+    __syncthreads();
+    unsigned long long p = s_part[threadIdx.x];
+    for (uint32_t j = j0; j < j1; ++j) {
+        start[j] = p;
+        p += count[j];
+    }
+}
+
+template <typename K>
+__global__ void batch_bucket_kernel(const K *__restrict__ Q, const uint32_t *__restrict__ qinst, uint64_t q,
+                                    uint32_t num, unsigned long long *__restrict__ cursor, K *__restrict__ sq,
+                                    uint32_t *__restrict__ sinst, uint64_t *__restrict__ sidx) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < q; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = qinst[i];
+        if (j >= num) continue;
+        const unsigned long long p = atomicAdd(&cursor[j], 1ull);
+        sq[p] = Q[i];
+        sinst[p] = j;
+        sidx[p] = i;
+    }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kBatchThreads)
+batch_query_kernel(const K *__restrict__ keys, const BatchInst *__restrict__ inst, const K *__restrict__ sq,
+                   const uint32_t *__restrict__ sinst, const uint64_t *__restrict__ sidx,
+                   const unsigned long long *__restrict__ nvalid, uint32_t chunk,
+                   const uint32_t *__restrict__ pin_levels, uint32_t pin_cap, uint64_t *__restrict__ ans) {
+    const uint64_t q = *nvalid;  // queries with a valid instance id (sorted first)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *sm = reinterpret_cast<K *>(smem_raw);
+    __shared__ uint32_t s_j, s_one;
+    __shared__ uint64_t s_P;
+    const uint64_t nchunks = (q + chunk - 1) / chunk;
+    for (uint64_t ck = blockIdx.x; ck < nchunks; ck += gridDim.x) {
+        const uint64_t q0 = ck * chunk, q1 = min(q, q0 + chunk);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_j = sinst[q0];
+            s_one = sinst[q1 - 1] == s_j;
+            uint64_t P = 0;
+            if (s_one) {
+                const BtreeStream &S = inst[s_j].S;
+                const uint32_t cls = S.g.n ? bit_length(S.g.n) - 1 : 0;
+                const uint32_t L = pin_levels[cls < kMaxClass ? cls : kMaxClass - 1];
+                const uint32_t LL = L < S.g.h + 1 ? L : S.g.h + 1;
+                P = L ? min(S.g.n, S.g.pw[LL] - 1) : 0;
+                if (P > pin_cap) P = 0;
+            }
+            s_P = P;
+        }
+        __syncthreads();
+        const uint64_t P = s_P;
+        if (P) {
+            const K *A = keys + inst[s_j].off;
+            for (uint64_t x = threadIdx.x; x < P; x += blockDim.x) sm[x] = __ldg(A + x);
+            __syncthreads();
+        }
+        for (uint64_t i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+            const uint32_t j = sinst[i];
+            const BtreeStream &S = inst[j].S;
+            const K *A = keys + inst[j].off;
+            const uint64_t n = S.g.n, b = S.g.b;
+            const uint64_t PP = (s_one && j == s_j) ? P : 0;
+            const K qv = sq[i];
+            uint64_t node = 0, res = n;
+            const uint64_t cmax = (n + 1) / (b + 1);
+            while (node < n) {
+                const uint64_t valid = min(b, n - node);
+                uint32_t lt = 0;
+                for (uint64_t s = 0; s < valid; ++s) {
+                    const uint64_t p = node + s;
+                    const K cur = p < PP ? sm[p] : __ldg(A + p);
+                    lt += cur < qv;
+                }
+                if (lt < valid) {
+                    const uint64_t p = node + lt;
+                    const K at = p < PP ? sm[p] : __ldg(A + p);
+                    if (at == qv) {
+                        res = p;
+                        break;
+                    }
+                }
+                if (node + 1 > cmax) break;
+                node = (node + 1) * (b + 1) + (uint64_t)lt * b - 1;
+            }
+            ans[sidx[i]] = res;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- host
+static int batch_sms() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+static void default_tuning(tl_batch_plan_impl &P) {
+    for (int c = 0; c < kMaxClass; ++c) {
+        P.tile_keys[c] = (uint32_t)(32768 / P.key_bytes);
+        P.pin_levels[c] = 3;
+    }
+    P.query_chunk = 2048;
+}
+
+static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStream_t st) {
+    uint32_t *d_tk = nullptr;
+    BatchTotals *d_tot = nullptr;
+    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_tk), sizeof(P.tile_keys), st));
+    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_tot), sizeof(BatchTotals), st));
+    TL_CUDA_TRY(cudaMemcpyAsync(d_tk, P.tile_keys, sizeof(P.tile_keys), cudaMemcpyHostToDevice, st));
+    batch_setup_kernel<<<1, 256, 0, st>>>(dev_offsets, P.num, P.b, FastDiv64(P.b + 1), FastDiv32((uint32_t)(P.b + 1)),
+                                           d_tk, P.inst, d_tot);
+    TL_CUDA_TRY(cudaGetLastError());
+    int64_t last = 0;
+    TL_CUDA_TRY(cudaMemcpyAsync(&P.tot, d_tot, sizeof(BatchTotals), cudaMemcpyDeviceToHost, st));
+    TL_CUDA_TRY(cudaMemcpyAsync(&last, dev_offsets + P.num, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    TL_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFreeAsync(d_tk, st);
+    cudaFreeAsync(d_tot, st);
+    P.total_keys = (uint64_t)last;
+    auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
+    P.off_flags = al(P.tot.scratch * P.key_bytes);
+    P.off_done = P.off_flags + al(P.tot.tiles * sizeof(unsigned int));
+    P.off_ctrl = P.off_done + al((uint64_t)P.num * sizeof(unsigned int));
+    P.ws_bytes = P.off_ctrl + al(sizeof(Ctrl));
+    return TL_SUCCESS;
+}
+
+int batch_plan_create(const int64_t *dev_offsets, uint32_t num, uint64_t b, uint32_t key_bytes, cudaStream_t st,
+                      tl_batch_plan **out) {
+    if (!dev_offsets || !out || num == 0 || num > (1u << 24) || b == 0 || b >= (1u << 20) ||
+        (key_bytes != 4 && key_bytes != 8))
+        return TL_ERROR_INVALID_VALUE;
+    auto *P = new tl_batch_plan_impl;
+    P->num = num;
+    P->b = b;
+    P->key_bytes = key_bytes;
+    default_tuning(*P);
+    if (cudaMalloc(reinterpret_cast<void **>(&P->inst), (size_t)num * sizeof(BatchInst)) != cudaSuccess) {
+        delete P;
+        return TL_ERROR_OUT_OF_MEMORY;
+    }
+    int rc = build_plan(*P, dev_offsets, st);
+    if (rc) {
+        cudaFree(P->inst);
+        delete P;
+        return rc;
+    }
+    *out = reinterpret_cast<tl_batch_plan *>(P);
+    return TL_SUCCESS;
+}
+
+int batch_plan_destroy(tl_batch_plan *plan) {
+    if (!plan) return TL_ERROR_INVALID_VALUE;
+    auto *P = reinterpret_cast<tl_batch_plan_impl *>(plan);
+    cudaFree(P->inst);
+    delete P;
+    return TL_SUCCESS;
+}
+
+int batch_workspace_bytes(const tl_batch_plan *plan, uint64_t *bytes) {
+    if (!plan || !bytes) return TL_ERROR_INVALID_VALUE;
+    *bytes = reinterpret_cast<const tl_batch_plan_impl *>(plan)->ws_bytes;
+    return TL_SUCCESS;
+}
+
+template <typename K>
+static int launch_batch_permute(const tl_batch_plan_impl &P, K *keys, char *ws, cudaStream_t st, int threads) {
+    K *scr = reinterpret_cast<K *>(ws);
+    unsigned int *flags = reinterpret_cast<unsigned int *>(ws + P.off_flags);
+    unsigned int *done = reinterpret_cast<unsigned int *>(ws + P.off_done);
+    Ctrl *ctrl = reinterpret_cast<Ctrl *>(ws + P.off_ctrl);
+    // flags, done counters and the control block are contiguous: one memset, no
+    // host-to-device copy, so the launch can be captured in a CUDA graph
+    TL_CUDA_TRY(cudaMemsetAsync(flags, 0, P.ws_bytes - P.off_flags, st));
+    WaitCfg wc;
+    wc.flag_value = 1;
+    wc.wait_value = debug_force_timeout() ? 0xFFFFFFFFu : 1u;
+    wc.spin_limit = debug_spin_limit();
+    const size_t smem = (size_t)P.tot.max_tile * sizeof(K) + 16;
+    auto kern = batch_permute_kernel<K>;
+    TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    const uint64_t work = P.tot.tiles + P.tot.chunks;
+    if (work == 0) return TL_SUCCESS;
+    const uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * batch_sms(), work);
+    kern<<<(unsigned)grid, threads, smem, st>>>(keys, scr, P.inst, P.num, P.tot, ctrl, wc, flags, done);
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
+int batch_permute(const tl_batch_plan *plan, void *dev_keys, void *dev_ws, uint64_t ws_bytes, cudaStream_t st) {
+    if (!plan || !dev_keys || !dev_ws) return TL_ERROR_INVALID_VALUE;
+    const auto &P = *reinterpret_cast<const tl_batch_plan_impl *>(plan);
+    if (ws_bytes < P.ws_bytes) return TL_ERROR_WORKSPACE_TOO_SMALL;
+    if (reinterpret_cast<uintptr_t>(dev_ws) % 256 || reinterpret_cast<uintptr_t>(dev_keys) % P.key_bytes)
+        return TL_ERROR_INVALID_VALUE;
+    char *ws = static_cast<char *>(dev_ws);
+    return P.key_bytes == 8 ? launch_batch_permute<uint64_t>(P, static_cast<uint64_t *>(dev_keys), ws, st, P.threads)
+                            : launch_batch_permute<uint32_t>(P, static_cast<uint32_t *>(dev_keys), ws, st, P.threads);
+}
+
+int batch_status(const tl_batch_plan *plan, const void *dev_ws, cudaStream_t st) {
+    if (!plan || !dev_ws) return TL_ERROR_INVALID_VALUE;
+    const auto &P = *reinterpret_cast<const tl_batch_plan_impl *>(plan);
+    const Ctrl *ctrl = reinterpret_cast<const Ctrl *>(static_cast<const char *>(dev_ws) + P.off_ctrl);
+    unsigned int err = 0;
+    int rc = read_error_word(&ctrl->error, &err, st);
+    if (rc) return rc;
+    return err ? TL_ERROR_TIMEOUT : TL_SUCCESS;
+}
+
+int batch_query_workspace_bytes(const tl_batch_plan *plan, uint64_t q, uint64_t *bytes) {
+    if (!plan || !bytes) return TL_ERROR_INVALID_VALUE;
+    const auto &P = *reinterpret_cast<const tl_batch_plan_impl *>(plan);
+    auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
+    *bytes = al((uint64_t)P.num * 4) + al(((uint64_t)P.num + 1) * 8) + al(q * P.key_bytes) + al(q * 4) + al(q * 8);
+    return TL_SUCCESS;
+}
+
+template <typename K>
+static int launch_batch_query(const tl_batch_plan_impl &P, const K *keys, const K *Q, const uint32_t *qinst,
+                              uint64_t q, uint64_t *ans, char *ws, cudaStream_t st) {
+    auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
+    unsigned int *count = reinterpret_cast<unsigned int *>(ws);
+    unsigned long long *start = reinterpret_cast<unsigned long long *>(ws + al((uint64_t)P.num * 4));
+    K *sq = reinterpret_cast<K *>(reinterpret_cast<char *>(start) + al(((uint64_t)P.num + 1) * 8));
+    uint32_t *sinst = reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(sq) + al(q * sizeof(K)));
+    uint64_t *sidx = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(sinst) + al(q * 4));
+    const int sms = batch_sms();
+    const unsigned g = (unsigned)std::min<uint64_t>((q + 255) / 256, (uint64_t)sms * 8);
+    TL_CUDA_TRY(cudaMemsetAsync(count, 0, (size_t)P.num * 4, st));
+    // queries whose instance id is out of range answer 0 (their answers are
+    // written here, the valid ones by the query kernel)
+    TL_CUDA_TRY(cudaMemsetAsync(ans, 0, q * 8, st));
+    batch_hist_kernel<<<g, 256, 0, st>>>(qinst, q, P.num, count);
+    batch_scan_kernel<<<1, 1024, 0, st>>>(count, P.num, start);
+    batch_bucket_kernel<K><<<g, 256, 0, st>>>(Q, qinst, q, P.num, start, sq, sinst, sidx);
+    TL_CUDA_TRY(cudaGetLastError());
+    // after the bucket pass start[j] holds the end of bucket j; the query kernel
+    // only needs the sorted arrays.  Valid queries: start[num] (read on device).
+    const uint32_t pin_cap = (uint32_t)(48 * 1024 / sizeof(K));
+    const size_t smem = (size_t)pin_cap * sizeof(K);
+    auto kern = batch_query_kernel<K>;
+    TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    uint32_t *d_pin = nullptr;
+    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_pin), sizeof(P.pin_levels), st));
+    TL_CUDA_TRY(cudaMemcpyAsync(d_pin, P.pin_levels, sizeof(P.pin_levels), cudaMemcpyHostToDevice, st));
+    int per_sm = 0;
+    TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchThreads, smem));
+    const uint64_t chunks = (q + P.query_chunk - 1) / P.query_chunk;
+    const unsigned grid = (unsigned)std::min<uint64_t>(chunks, (uint64_t)std::max(per_sm, 1) * sms);
+    kern<<<grid, kBatchThreads, smem, st>>>(keys, P.inst, sq, sinst, sidx, start + P.num, P.query_chunk, d_pin,
+                                           pin_cap, ans);
+    cudaFreeAsync(d_pin, st);
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
+int batch_query(const tl_batch_plan *plan, const void *dev_keys, const void *dev_queries, const uint32_t *dev_inst,
+                uint64_t q, uint64_t *dev_answers, void *dev_ws, uint64_t ws_bytes, cudaStream_t st, float *ms) {
+    if (!plan || (q && (!dev_keys || !dev_queries || !dev_inst || !dev_answers || !dev_ws)))
+        return TL_ERROR_INVALID_VALUE;
+    const auto &P = *reinterpret_cast<const tl_batch_plan_impl *>(plan);
+    uint64_t need = 0;
+    batch_query_workspace_bytes(plan, q, &need);
+    if (ws_bytes < need) return TL_ERROR_WORKSPACE_TOO_SMALL;
+    if (q == 0) return TL_SUCCESS;
+    EventTimer timer(ms != nullptr, st);
+    timer.start();
+    char *ws = static_cast<char *>(dev_ws);
+    int rc = P.key_bytes == 8
+                 ? launch_batch_query<uint64_t>(P, static_cast<const uint64_t *>(dev_keys),
+                                                static_cast<const uint64_t *>(dev_queries), dev_inst, q, dev_answers, ws, st)
+                 : launch_batch_query<uint32_t>(P, static_cast<const uint32_t *>(dev_keys),
+                                                static_cast<const uint32_t *>(dev_queries), dev_inst, q, dev_answers, ws, st);
+    timer.stop();
+    if (rc) return rc;
+    if (ms) {
+        rc = sync_and_check(st);
+        if (rc) return rc;
+        *ms = timer.elapsed();
+    }
+    return TL_SUCCESS;
+}
+
+int batch_set_tuning(tl_batch_plan *plan, const uint32_t *tile_keys, const uint32_t *pin_levels, uint32_t query_chunk,
+                     uint32_t threads, const int64_t *dev_offsets, cudaStream_t st) {
+    if (!plan) return TL_ERROR_INVALID_VALUE;
+    auto &P = *reinterpret_cast<tl_batch_plan_impl *>(plan);
+    if (tile_keys) {
+        for (int c = 0; c < kMaxClass; ++c) {
+            const uint32_t t = tile_keys[c];
+            if (t < 256 || t * P.key_bytes > 96 * 1024 || t % 16) return TL_ERROR_INVALID_VALUE;
+        }
+        memcpy(P.tile_keys, tile_keys, sizeof(P.tile_keys));
+        if (!dev_offsets) return TL_ERROR_INVALID_VALUE;
+        int rc = build_plan(P, dev_offsets, st);
+        if (rc) return rc;
+    }
+    if (pin_levels) memcpy(P.pin_levels, pin_levels, sizeof(P.pin_levels));
+    if (query_chunk) P.query_chunk = query_chunk;
+    if (threads) {
+        if (threads != 256 && threads != 512) return TL_ERROR_INVALID_VALUE;
+        P.threads = threads;
+    }
+    return TL_SUCCESS;
+}
+
+int batch_get_tuning(const tl_batch_plan *plan, uint32_t *tile_keys, uint32_t *pin_levels, uint32_t *query_chunk,
+                     uint32_t *threads) {
+    if (!plan) return TL_ERROR_INVALID_VALUE;
+    const auto &P = *reinterpret_cast<const tl_batch_plan_impl *>(plan);
+    if (tile_keys) memcpy(tile_keys, P.tile_keys, sizeof(P.tile_keys));
+    if (pin_levels) memcpy(pin_levels, P.pin_levels, sizeof(P.pin_levels));
+    if (query_chunk) *query_chunk = P.query_chunk;
+    if (threads) *threads = P.threads;
+    return TL_SUCCESS;
+}
+
+// Size classes present in the batch (floor(log2 n_j)) and the keys in each,
+// read back from the plan (host).
+static int batch_class_keys(const tl_batch_plan_impl &P, std::vector<uint64_t> &keys_per_class) {
+    std::vector<BatchInst> h(P.num);
+    TL_CUDA_TRY(cudaMemcpy(h.data(), P.inst, (size_t)P.num * sizeof(BatchInst), cudaMemcpyDeviceToHost));
+    keys_per_class.assign(kMaxClass, 0);
+    for (const auto &I : h) {
+        const uint64_t n = I.S.g.n;
+        const uint32_t c = n ? bit_length(n) - 1 : 0;
+        keys_per_class[c < kMaxClass ? c : kMaxClass - 1] += n;
+    }
+    return TL_SUCCESS;
+}
+
+// Coordinate-descent autotuner.  Permutation: the block size, then per size class
+// (largest classes first) the tile size, each candidate timed on the whole batch
+// (the sorted input restored from a copy before every trial).  Queries: the
+// work-item size, then per size class the number of top levels pinned in shared
+// memory.  The plan keeps the best values; the keys are left sorted.
+int batch_autotune(tl_batch_plan *plan, const int64_t *dev_offsets, void *dev_keys, const void *dev_queries,
+                   const uint32_t *dev_inst, uint64_t q, cudaStream_t st, char *report, size_t report_len) {
+    if (!plan || !dev_offsets || !dev_keys) return TL_ERROR_INVALID_VALUE;
+    auto &P = *reinterpret_cast<tl_batch_plan_impl *>(plan);
+    const size_t kbytes = (size_t)P.total_keys * P.key_bytes;
+    char *pristine = nullptr, *ws = nullptr;
+    int rc = TL_SUCCESS;
+    std::vector<uint64_t> cls_keys;
+    rc = batch_class_keys(P, cls_keys);
+    if (rc) return rc;
+    if (cudaMalloc(reinterpret_cast<void **>(&pristine), kbytes) != cudaSuccess) return TL_ERROR_OUT_OF_MEMORY;
+    TL_CUDA_TRY(cudaMemcpyAsync(pristine, dev_keys, kbytes, cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    uint64_t ws_cap = 0;
+    auto ensure_ws = [&](uint64_t need) -> int {
+        if (need <= ws_cap) return TL_SUCCESS;
+        if (ws) cudaFree(ws);
+        ws = nullptr;
+        ws_cap = 0;
+        if (cudaMalloc(reinterpret_cast<void **>(&ws), need) != cudaSuccess) return TL_ERROR_OUT_OF_MEMORY;
+        ws_cap = need;
+        return TL_SUCCESS;
+    };
+    auto time_permute = [&](float &best) -> int {
+        float total = 0.f;
+        for (int rep = 0; rep < 3; ++rep) {
+            TL_CUDA_TRY(cudaMemcpyAsync(dev_keys, pristine, kbytes, cudaMemcpyDeviceToDevice, st));
+            int r = ensure_ws(P.ws_bytes);
+            if (r) return r;
+            cudaEventRecord(e0, st);
+            r = batch_permute(plan, dev_keys, ws, ws_cap, st);
+            if (r) return r;
+            cudaEventRecord(e1, st);
+            TL_CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep) total += ms;  // first repetition warms up
+        }
+        best = total / 2;
+        return TL_SUCCESS;
+    };
+    const uint32_t tiles[3] = {(uint32_t)(8192 / P.key_bytes), (uint32_t)(16384 / P.key_bytes),
+                               (uint32_t)(32768 / P.key_bytes)};
+    float cur = 0.f;
+    rc = time_permute(cur);
+    // block size
+    for (uint32_t th : {512u, 256u}) {
+        if (rc) break;
+        const uint32_t keep = P.threads;
+        P.threads = th;
+        float ms = 0.f;
+        rc = time_permute(ms);
+        if (!rc && ms < cur) cur = ms; else P.threads = keep;
+    }
+    // tile size per class, largest classes first
+    std::vector<int> order;
+    for (int c = 0; c < kMaxClass; ++c)
+        if (cls_keys[c]) order.push_back(c);
+    std::sort(order.begin(), order.end(), [&](int a, int b2) { return cls_keys[a] > cls_keys[b2]; });
+    for (int c : order) {
+        if (rc) break;
+        const uint32_t keep = P.tile_keys[c];
+        uint32_t best_t = keep;
+        for (uint32_t t : tiles) {
+            if (t == keep) continue;
+            P.tile_keys[c] = t;
+            rc = build_plan(P, dev_offsets, st);
+            if (rc) break;
+            float ms = 0.f;
+            rc = time_permute(ms);
+            if (rc) break;
+            if (ms < cur) {
+                cur = ms;
+                best_t = t;
+            }
+        }
+        P.tile_keys[c] = best_t;
+        if (!rc) rc = build_plan(P, dev_offsets, st);
+    }
+    float qcur = -1.f;
+    if (!rc && q && dev_queries && dev_inst) {
+        // a permuted copy for the query trials
+        TL_CUDA_TRY(cudaMemcpyAsync(dev_keys, pristine, kbytes, cudaMemcpyDeviceToDevice, st));
+        rc = ensure_ws(P.ws_bytes);
+        if (!rc) rc = batch_permute(plan, dev_keys, ws, ws_cap, st);
+        uint64_t qneed = 0;
+        batch_query_workspace_bytes(plan, q, &qneed);
+        char *qws = nullptr;
+        uint64_t *ans = nullptr;
+        if (!rc && (cudaMalloc(reinterpret_cast<void **>(&qws), qneed) != cudaSuccess ||
+                    cudaMalloc(reinterpret_cast<void **>(&ans), q * 8) != cudaSuccess))
+            rc = TL_ERROR_OUT_OF_MEMORY;
+        auto time_query = [&](float &out) -> int {
+            float total = 0.f;
+            for (int rep = 0; rep < 3; ++rep) {
+                float ms = 0.f;
+                int r = batch_query(plan, dev_keys, dev_queries, dev_inst, q, ans, qws, qneed, st, &ms);
+                if (r) return r;
+                if (rep) total += ms;
+            }
+            out = total / 2;
+            return TL_SUCCESS;
+        };
+        if (!rc) rc = time_query(qcur);
+        for (uint32_t ch : {1024u, 4096u}) {
+            if (rc) break;
+            const uint32_t keep = P.query_chunk;
+            P.query_chunk = ch;
+            float ms = 0.f;
+            rc = time_query(ms);
+            if (!rc && ms < qcur) qcur = ms; else P.query_chunk = keep;
+        }
+        for (int c : order) {
+            if (rc) break;
+            const uint32_t keep = P.pin_levels[c];
+            uint32_t best_l = keep;
+            for (uint32_t L : {0u, 2u, 4u}) {
+                if (L == keep) continue;
+                P.pin_levels[c] = L;
+                float ms = 0.f;
+                rc = time_query(ms);
+                if (rc) break;
+                if (ms < qcur) {
+                    qcur = ms;
+                    best_l = L;
+                }
+            }
+            P.pin_levels[c] = best_l;
+        }
+        if (qws) cudaFree(qws);
+        if (ans) cudaFree(ans);
+    }
+    cudaMemcpyAsync(dev_keys, pristine, kbytes, cudaMemcpyDeviceToDevice, st);
+    cudaStreamSynchronize(st);
+    cudaFree(pristine);
+    if (ws) cudaFree(ws);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (report && report_len) {
+        std::string r = "{\"threads\":" + std::to_string(P.threads) + ",\"query_chunk\":" +
+                        std::to_string(P.query_chunk) + ",\"permute_ms\":" + std::to_string(cur) +
+                        ",\"query_ms\":" + std::to_string(qcur) + ",\"classes\":{";
+        bool first = true;
+        for (int c : order) {
+            r += (first ? "" : ",") + std::string("\"") + std::to_string(c) + "\":{\"keys\":" +
+                 std::to_string(cls_keys[c]) + ",\"tile_keys\":" + std::to_string(P.tile_keys[c]) +
+                 ",\"pin_levels\":" + std::to_string(P.pin_levels[c]) + "}";
+            first = false;
+        }
+        r += "}}";
+        snprintf(report, report_len, "%s", r.c_str());
+    }
+    return rc;
+}
+
+}  // namespace tl

@@ -6,6 +6,8 @@
 
 #include "geometry.cuh"
 #include "internal.h"
+#include "learned.h"
+#include "batched.h"
 
 namespace tl {
 
@@ -102,6 +104,16 @@ int tl_last_cuda_error(void) { return t_last_cuda_error; }
 int tl_debug_set_wait(unsigned int spin_limit, int force_timeout) {
     debug_set_wait(spin_limit, force_timeout);
     return TL_SUCCESS;
+}
+
+int tl_debug_struct_size(int which) {
+    switch (which) {
+        case 0: return (int)sizeof(tl_veb_table);
+        case 1: return (int)sizeof(tl_rank_model);
+        case 2: return (int)sizeof(tl_rank_leaf);
+        case 3: return (int)sizeof(tl_rank_train_config);
+        default: return -1;
+    }
 }
 
 // Test hook: which B-tree schedule the permutation uses (0: right-to-left
@@ -203,6 +215,56 @@ int tl_build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_
         td = id;
     }
     return TL_SUCCESS;
+}
+
+int tl_batch_plan_create(const int64_t *off, uint32_t num, uint64_t b, uint32_t kb, void *stream,
+                         tl_batch_plan **plan) {
+    return batch_plan_create(off, num, b, kb, S(stream), plan);
+}
+int tl_batch_plan_destroy(tl_batch_plan *plan) { return batch_plan_destroy(plan); }
+int tl_batch_workspace_bytes(const tl_batch_plan *plan, uint64_t *bytes) { return batch_workspace_bytes(plan, bytes); }
+int tl_batch_permute(const tl_batch_plan *plan, void *keys, void *ws, uint64_t wsb, void *stream) {
+    return batch_permute(plan, keys, ws, wsb, S(stream));
+}
+int tl_batch_status(const tl_batch_plan *plan, const void *ws, void *stream) {
+    return batch_status(plan, ws, S(stream));
+}
+int tl_batch_query_workspace_bytes(const tl_batch_plan *plan, uint64_t q, uint64_t *bytes) {
+    return batch_query_workspace_bytes(plan, q, bytes);
+}
+int tl_batch_query(const tl_batch_plan *plan, const void *keys, const void *Q, const uint32_t *inst, uint64_t q,
+                   uint64_t *ans, void *ws, uint64_t wsb, void *stream, float *ms) {
+    return batch_query(plan, keys, Q, inst, q, ans, ws, wsb, S(stream), ms);
+}
+int tl_batch_set_tuning(tl_batch_plan *plan, const uint32_t *tile_keys, const uint32_t *pin_levels,
+                        uint32_t query_chunk, uint32_t threads, const int64_t *off, void *stream) {
+    return batch_set_tuning(plan, tile_keys, pin_levels, query_chunk, threads, off, S(stream));
+}
+int tl_batch_get_tuning(const tl_batch_plan *plan, uint32_t *tile_keys, uint32_t *pin_levels, uint32_t *query_chunk,
+                        uint32_t *threads) {
+    return batch_get_tuning(plan, tile_keys, pin_levels, query_chunk, threads);
+}
+int tl_batch_autotune(tl_batch_plan *plan, const int64_t *off, void *keys, const void *Q, const uint32_t *inst,
+                      uint64_t q, void *stream, char *report, uint64_t report_len) {
+    return batch_autotune(plan, off, keys, Q, inst, q, S(stream), report, (size_t)report_len);
+}
+
+int tl_rank_model_train(const uint64_t *keys, uint64_t n, const tl_rank_train_config *cfg, tl_rank_model *model,
+                        tl_rank_leaf *leaves, void *stream) {
+    return rank_model_train(keys, n, cfg, model, leaves, S(stream));
+}
+int tl_rank_model_predict(const tl_rank_model *model, const tl_rank_leaf *leaves, const uint64_t *keys, uint64_t q,
+                          uint64_t *rank, uint32_t *eps, void *stream) {
+    return rank_model_predict(model, leaves, keys, q, rank, eps, S(stream));
+}
+int tl_rank_model_gradient(const tl_rank_model *model, const float *dx, const float *dy, uint32_t m, float *grad,
+                           float *loss, void *stream) {
+    return rank_model_gradient(model, dx, dy, m, grad, loss, S(stream));
+}
+int tl_query_btree_learned_u64(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank_model *model,
+                               const tl_rank_leaf *leaves, const uint64_t *Q, uint64_t q, uint64_t *ans,
+                               unsigned long long *stats, void *stream, float *ms) {
+    return query_btree_learned(A, n, b, model, leaves, Q, q, ans, stats, S(stream), ms);
 }
 
 #define TL_Q(NAME, K, KB, LAYOUT, ...)                                                                  \

@@ -35,7 +35,7 @@ struct BtreeGeom {
     uint64_t pw[48];      // (b+1)^k for k <= h + 1 (saturating)
 };
 
-__host__ inline BtreeGeom make_btree_geom(uint64_t n, uint64_t b) {
+TL_HD BtreeGeom make_btree_geom(uint64_t n, uint64_t b) {
     BtreeGeom g;
     g.n = n;
     g.b = b;
@@ -65,6 +65,15 @@ __host__ inline BtreeGeom make_btree_geom(uint64_t n, uint64_t b) {
 // Position of top rank c in a perfect B-tree of H levels (levels counted from the
 // root).  The level of c is the number of times b+1 divides c+1.
 TL_HD uint64_t btree_perfect_pos(const BtreeGeom &g, const FastDiv64 &fd, uint64_t c, uint32_t H) {
+    if (g.b == 1) {  // binary tree: the level is the number of trailing zero bits of c+1
+        const uint64_t x1 = c + 1;
+#ifdef __CUDA_ARCH__
+        const uint32_t k = (uint32_t)__ffsll((long long)x1) - 1;
+#else
+        const uint32_t k = (uint32_t)__builtin_ctzll(x1);
+#endif
+        return g.pw[H - 1 - k] - 1 + (x1 >> (k + 1));
+    }
     uint64_t x = c + 1, q, rem;
     uint32_t k = 0;
     for (;;) {

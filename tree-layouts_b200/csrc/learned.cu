@@ -1,0 +1,724 @@
+// Learned-start exact B-tree query (no counterpart in the reference).
+//
+// A two-stage rank model predicts the sorted rank of a key: an FP32 root MLP
+// 1 -> 32 -> 32 -> 1 over the normalised key picks one of L linear leaf segments;
+// the leaf maps the key to a rank and carries eps, the largest rank error over
+// the keys it was fitted on.  The query starts its B-tree descent at the deepest
+// subtree whose in-order rank range covers [rank - eps, rank + eps].  Answers
+// stay exact: a hit is a hit; a miss is only accepted when the subtree held keys
+// on both sides of the query (so the key, if present, would be in it); every
+// other case falls back to the plain search from the root.
+//
+// Everything here is hand-written CUDA: the training batch sampler, the forward
+// and backward passes (per-block partial gradients reduced in a fixed order, so
+// training is deterministic), Adam, the leaf fit, the eps pass, inference and
+// the query.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "geometry.cuh"
+#include "internal.h"
+#include "learned.h"
+
+namespace tl {
+
+constexpr int H = TL_RMI_HIDDEN;
+constexpr int kParams = H + H + H * H + H + H + 1;  // w1 b1 w2 b2 w3 b3
+constexpr int kTrainThreads = 64;                  // samples per training block
+
+struct ModelParams {  // kernel-parameter copy of the root network (constant bank)
+    float w1[H], b1[H], w2[H][H], b2[H], w3[H], b3;
+    float2 w2p[H][H / 2];  // w2p[i][k] = (w2[2k][i], w2[2k+1][i]): the hidden layer two outputs at a time
+    float2 b2p[H / 2], w3p[H / 2];
+    float x_lo, x_scale;
+    uint32_t log_feature, num_leaves;
+};
+
+static ModelParams to_params(const tl_rank_model &m) {
+    ModelParams p;
+    memcpy(p.w1, m.w1, sizeof p.w1);
+    memcpy(p.b1, m.b1, sizeof p.b1);
+    memcpy(p.w2, m.w2, sizeof p.w2);
+    memcpy(p.b2, m.b2, sizeof p.b2);
+    memcpy(p.w3, m.w3, sizeof p.w3);
+    p.b3 = m.b3;
+    for (int i = 0; i < H; ++i)
+        for (int k = 0; k < H / 2; ++k) p.w2p[i][k] = make_float2(m.w2[2 * k][i], m.w2[2 * k + 1][i]);
+    for (int k = 0; k < H / 2; ++k) {
+        p.b2p[k] = make_float2(m.b2[2 * k], m.b2[2 * k + 1]);
+        p.w3p[k] = make_float2(m.w3[2 * k], m.w3[2 * k + 1]);
+    }
+    p.x_lo = (float)m.x_lo;
+    p.x_scale = (float)m.x_scale;
+    p.log_feature = m.log_feature;
+    p.num_leaves = m.num_leaves;
+    return p;
+}
+
+// Normalised feature of a key, in [0, 1] over the trained key range:
+// f = log2(key + 1) (FP32) or the key itself, x = (f - x_lo) * x_scale clamped.
+// Training, the segment fit and the queries all evaluate it with this one
+// function (feature_of is the same arithmetic for training's parameter struct).
+__device__ __forceinline__ float feature_x(uint32_t log_feature, float x_lo, float x_scale, uint64_t key) {
+    const float f = log_feature ? log2f((float)key + 1.0f) : (float)key;
+    const float x = (f - x_lo) * x_scale;
+    return x < 0.f ? 0.f : (x > 1.f ? 1.f : x);
+}
+
+__device__ __forceinline__ float feature(const ModelParams &p, uint64_t key) {
+    return feature_x(p.log_feature, p.x_lo, p.x_scale, key);
+}
+
+// Root network output (predicted rank / n).  The hidden layer runs two output
+// units per packed FP32x2 FMA (sm_100's FFMA2), each lane a plain fmaf chain in
+// the same input order.
+__device__ __forceinline__ float root_forward(const ModelParams &p, float x) {
+    float2 acc[H / 2];
+#pragma unroll
+    for (int k = 0; k < H / 2; ++k) acc[k] = p.b2p[k];
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        const float h = fmaxf(fmaf(p.w1[i], x, p.b1[i]), 0.f);
+        const float2 hh = make_float2(h, h);
+#pragma unroll
+        for (int k = 0; k < H / 2; ++k) acc[k] = __ffma2_rn(p.w2p[i][k], hh, acc[k]);
+    }
+    float2 o = make_float2(p.b3, 0.f);
+#pragma unroll
+    for (int k = 0; k < H / 2; ++k)
+        o = __ffma2_rn(p.w3p[k], make_float2(fmaxf(acc[k].x, 0.f), fmaxf(acc[k].y, 0.f)), o);
+    return o.x + o.y;
+}
+
+__device__ __forceinline__ uint32_t leaf_of(const ModelParams &p, float out) {
+    float f = out * (float)p.num_leaves;
+    if (!(f > 0.f)) return 0;  // also catches NaN
+    uint32_t l = (uint32_t)f;
+    return l < p.num_leaves ? l : p.num_leaves - 1;
+}
+
+// Leaf-only ablation: the root network replaced by the identity.
+__device__ __forceinline__ float root_eval(const ModelParams &p, float x, bool use_net) {
+    return use_net ? root_forward(p, x) : x;
+}
+
+// Rank prediction of a segment, clamped to [0, n).
+__device__ __forceinline__ uint64_t leaf_predict(const tl_rank_leaf &lf, uint64_t key, uint64_t n) {
+    float off = key > lf.kmin ? (float)(key - lf.kmin) : 0.f;
+    float r = (float)lf.base + lf.slope * off;
+    if (!(r > 0.f)) return 0;
+    uint64_t ri = (uint64_t)(r + 0.5f);
+    return ri < n ? ri : n - 1;
+}
+
+// splitmix64 (Steele, Lea, Flood, OOPSLA 2014) for the training sampler.
+TL_HD uint64_t mix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// ---------------------------------------------------------------- training
+// Flat parameter order: w1[H] b1[H] w2[H][H] b2[H] w3[H] b3.
+// Per block: forward + backward of kTrainThreads samples with the current
+// weights (read from `w`, staged in shared memory), gradient of the mean
+// squared error over the batch summed over the block's samples in a fixed
+// order, written to partial[block][kParams].  Samples come either from (x, y)
+// arrays or from the sorted keys (rank drawn by a hash of (seed, index)).
+struct Feature {
+    float x_lo, x_scale;
+    uint32_t log_feature;
+};
+
+__device__ __forceinline__ float feature_of(const Feature &f, uint64_t key) {
+    return feature_x(f.log_feature, f.x_lo, f.x_scale, key);
+}
+
+__global__ void __launch_bounds__(kTrainThreads)
+rmi_grad_kernel(const float *__restrict__ w, Feature fe, const float *__restrict__ xs,
+                const float *__restrict__ ys, const uint64_t *__restrict__ keys, uint64_t n, uint64_t seed,
+                uint32_t m, float inv_m, float *__restrict__ partial, float *__restrict__ loss_partial) {
+    __shared__ float sw[kParams];
+    __shared__ float s_h1[kTrainThreads][H + 1];
+    __shared__ float s_h2[kTrainThreads][H + 1];
+    __shared__ float s_dz1[kTrainThreads][H + 1];
+    __shared__ float s_dz2[kTrainThreads][H + 1];
+    __shared__ float s_x[kTrainThreads];
+    __shared__ float s_dout[kTrainThreads];
+    __shared__ float s_loss[kTrainThreads];
+    const uint32_t t = threadIdx.x;
+    for (int k = t; k < kParams; k += kTrainThreads) sw[k] = w[k];
+    __syncthreads();
+    const float *w1 = sw, *b1 = sw + H, *w2 = sw + 2 * H, *b2 = sw + 2 * H + H * H, *w3 = b2 + H;
+    const float b3 = w3[H];
+    const uint64_t gi = (uint64_t)blockIdx.x * kTrainThreads + t;
+    const bool valid = gi < m;
+    float x = 0.f, y = 0.f;
+    if (valid) {
+        if (xs) {
+            x = xs[gi];
+            y = ys[gi];
+        } else {
+            const uint64_t r = mix64(seed ^ mix64(gi)) % n;
+            x = feature_of(fe, keys[r]);
+            y = ((float)r + 0.5f) / (float)n;
+        }
+    }
+    // forward; ReLU masks kept as bits, activations in shared memory
+    float h1[H];
+    uint32_t mask1 = 0, mask2 = 0;
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        const float z = fmaf(w1[i], x, b1[i]);
+        h1[i] = fmaxf(z, 0.f);
+        mask1 |= (z > 0.f ? 1u : 0u) << i;
+        s_h1[t][i] = h1[i];
+    }
+    float out = b3;
+    for (int j = 0; j < H; ++j) {
+        float a = b2[j];
+#pragma unroll
+        for (int i = 0; i < H; ++i) a = fmaf(w2[j * H + i], h1[i], a);
+        mask2 |= (a > 0.f ? 1u : 0u) << j;
+        const float h2 = fmaxf(a, 0.f);
+        s_h2[t][j] = h2;
+        out = fmaf(w3[j], h2, out);
+    }
+    // backward
+    const float diff = out - y;
+    const float dout = valid ? 2.f * diff * inv_m : 0.f;
+    s_loss[t] = valid ? diff * diff * inv_m : 0.f;
+    s_x[t] = x;
+    s_dout[t] = dout;
+#pragma unroll
+    for (int j = 0; j < H; ++j) s_dz2[t][j] = ((mask2 >> j) & 1u) ? dout * w3[j] : 0.f;
+    for (int i = 0; i < H; ++i) {
+        float dh = 0.f;
+#pragma unroll
+        for (int j = 0; j < H; ++j) dh = fmaf(s_dz2[t][j], w2[j * H + i], dh);
+        s_dz1[t][i] = ((mask1 >> i) & 1u) ? dh : 0.f;
+    }
+    __syncthreads();
+    // per-block gradient sums, fixed summation order over the block's samples
+    float *g = partial + (size_t)blockIdx.x * kParams;
+    for (int e = t; e < H * H; e += kTrainThreads) {  // dL/dw2[j][i] = sum_s dz2[s][j] h1[s][i]
+        const int j = e / H, i = e % H;
+        float acc = 0.f;
+        for (int s2 = 0; s2 < kTrainThreads; ++s2) acc = fmaf(s_dz2[s2][j], s_h1[s2][i], acc);
+        g[2 * H + e] = acc;
+    }
+    if (t < H) {
+        float gw1 = 0.f, gb1 = 0.f, gb2 = 0.f, gw3 = 0.f;
+        for (int s2 = 0; s2 < kTrainThreads; ++s2) {
+            gw1 = fmaf(s_dz1[s2][t], s_x[s2], gw1);
+            gb1 += s_dz1[s2][t];
+            gb2 += s_dz2[s2][t];
+            gw3 = fmaf(s_dout[s2], s_h2[s2][t], gw3);
+        }
+        g[t] = gw1;
+        g[H + t] = gb1;
+        g[2 * H + H * H + t] = gb2;
+        g[3 * H + H * H + t] = gw3;
+    }
+    if (t == 0) {
+        float gb3 = 0.f, l = 0.f;
+        for (int s2 = 0; s2 < kTrainThreads; ++s2) {
+            gb3 += s_dout[s2];
+            l += s_loss[s2];
+        }
+        g[4 * H + H * H] = gb3;
+        loss_partial[blockIdx.x] = l;
+    }
+}
+
+// Sums the per-block partials in block order (deterministic): grad[k], loss.
+__global__ void rmi_reduce_kernel(const float *__restrict__ partial, const float *__restrict__ loss_partial,
+                                  uint32_t blocks, float *__restrict__ grad, float *__restrict__ loss) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < kParams + 1; k += gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        if (k < kParams)
+            for (uint32_t b = 0; b < blocks; ++b) acc += partial[(size_t)b * kParams + k];
+        else
+            for (uint32_t b = 0; b < blocks; ++b) acc += loss_partial[b];
+        if (k < kParams) grad[k] = acc; else *loss = acc;
+    }
+}
+
+// Adam (Kingma & Ba, ICLR 2015) on the flat parameter vector.
+// With `monotone`, the weights of the three layers are projected onto w >= 0
+// after each step, which keeps the root non-decreasing in the key (biases stay
+// free): every segment then receives one contiguous key range.
+__device__ __forceinline__ bool is_weight(int k) {
+    return k < H || (k >= 2 * H && k < 2 * H + H * H) || (k >= 3 * H + H * H && k < 4 * H + H * H);
+}
+
+__global__ void rmi_adam_kernel(float *__restrict__ w, float *__restrict__ mom, float *__restrict__ vel,
+                                const float *__restrict__ grad, float lr, float b1, float b2, float eps,
+                                float c1, float c2, int monotone) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < kParams; k += gridDim.x * blockDim.x) {
+        const float g = grad[k];
+        mom[k] = b1 * mom[k] + (1.f - b1) * g;
+        vel[k] = b2 * vel[k] + (1.f - b2) * g * g;
+        float nw = w[k] - lr * (mom[k] / c1) / (sqrtf(vel[k] / c2) + eps);
+        if (monotone && is_weight(k)) nw = fmaxf(nw, 0.f);
+        w[k] = nw;
+    }
+}
+
+// ---------------------------------------------------------------- leaves
+// Each thread walks a contiguous run of sorted keys and emits one set of
+// atomics per change of leaf (the root is close to monotone, so runs are long).
+constexpr int kLeafChunk = 64;
+
+__global__ void leaf_extent_kernel(const ModelParams p, bool use_net, const uint64_t *__restrict__ keys,
+                                   uint64_t n, unsigned long long *kmin, unsigned long long *kmax,
+                                   unsigned long long *rmin, unsigned long long *rmax) {
+    const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c * kLeafChunk < n; c += nthr) {
+        const uint64_t s0 = c * kLeafChunk, s1 = min(n, s0 + kLeafChunk);
+        uint32_t cur = 0xFFFFFFFFu;
+        uint64_t lo_k = 0, hi_k = 0, lo_r = 0, hi_r = 0;
+        for (uint64_t s = s0; s <= s1; ++s) {
+            uint32_t l = 0xFFFFFFFFu;
+            uint64_t k = 0;
+            if (s < s1) {
+                k = keys[s];
+                l = leaf_of(p, root_eval(p, feature(p, k), use_net));
+            }
+            if (l != cur) {
+                if (cur != 0xFFFFFFFFu) {
+                    atomicMin(&kmin[cur], (unsigned long long)lo_k);
+                    atomicMax(&kmax[cur], (unsigned long long)hi_k);
+                    atomicMin(&rmin[cur], (unsigned long long)lo_r);
+                    atomicMax(&rmax[cur], (unsigned long long)hi_r);
+                }
+                cur = l;
+                lo_k = hi_k = k;
+                lo_r = hi_r = s;
+            } else {
+                lo_k = min(lo_k, k);
+                hi_k = max(hi_k, k);
+                lo_r = min(lo_r, s);
+                hi_r = max(hi_r, s);
+            }
+        }
+    }
+}
+
+// Linear segment through the extreme (key, rank) points of the segment's keys.
+__global__ void leaf_fit_kernel(uint32_t L, const unsigned long long *kmin, const unsigned long long *kmax,
+                                const unsigned long long *rmin, const unsigned long long *rmax,
+                                tl_rank_leaf *leaves) {
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < L; l += gridDim.x * blockDim.x) {
+        tl_rank_leaf lf;
+        lf.eps_lo = lf.eps_hi = 0;
+        if (kmin[l] > kmax[l]) {
+            lf.kmin = 0;
+            lf.base = 0;
+            lf.slope = 0.f;
+            lf.empty = 1;
+        } else {
+            lf.kmin = kmin[l];
+            lf.base = rmin[l];
+            const double dk = (double)(kmax[l] - kmin[l]);
+            lf.slope = dk > 0 ? (float)((double)(rmax[l] - rmin[l]) / dk) : 0.f;
+            lf.empty = 0;
+        }
+        leaves[l] = lf;
+    }
+}
+
+// The segment's error bounds: the largest over- and under-prediction over its
+// keys, computed with the inference arithmetic itself.
+__global__ void leaf_eps_kernel(const ModelParams p, bool use_net, const uint64_t *__restrict__ keys, uint64_t n,
+                                tl_rank_leaf *leaves) {
+    const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c * kLeafChunk < n; c += nthr) {
+        const uint64_t s0 = c * kLeafChunk, s1 = min(n, s0 + kLeafChunk);
+        uint32_t cur = 0xFFFFFFFFu, over = 0, under = 0;
+        for (uint64_t s = s0; s <= s1; ++s) {
+            uint32_t l = 0xFFFFFFFFu, eo = 0, eu = 0;
+            if (s < s1) {
+                const uint64_t k = keys[s];
+                l = leaf_of(p, root_eval(p, feature(p, k), use_net));
+                const uint64_t pr = leaf_predict(leaves[l], k, n);
+                const uint64_t d = pr > s ? pr - s : s - pr;
+                const uint32_t e = d > 0xFFFFFFFEull ? 0xFFFFFFFEu : (uint32_t)d;
+                if (pr > s) eo = e; else eu = e;
+            }
+            if (l != cur) {
+                if (cur != 0xFFFFFFFFu) {
+                    atomicMax(&leaves[cur].eps_lo, over);
+                    atomicMax(&leaves[cur].eps_hi, under);
+                }
+                cur = l;
+                over = eo;
+                under = eu;
+            } else {
+                over = max(over, eo);
+                under = max(under, eu);
+            }
+        }
+    }
+}
+
+__global__ void rmi_predict_kernel(const ModelParams p, bool use_net, const tl_rank_leaf *__restrict__ leaves,
+                                   const uint64_t *__restrict__ keys, uint64_t nq, uint64_t n,
+                                   uint64_t *__restrict__ rank, uint32_t *__restrict__ eps) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = keys[i];
+        const uint32_t l = leaf_of(p, root_eval(p, feature(p, k), use_net));
+        const tl_rank_leaf lf = leaves[l];
+        rank[i] = leaf_predict(lf, k, n);
+        if (eps) eps[i] = lf.empty ? 0xFFFFFFFFu : max(lf.eps_lo, lf.eps_hi);
+    }
+}
+
+// ---------------------------------------------------------------- learned query
+struct LearnedGeom {
+    BtreeGeom g;
+    FastDiv64 fd;
+};
+
+// In-order "gap" coordinates: the top tree's ni keys split the key space into
+// ni + 1 gaps; gap j holds leaf node j of the last level (if it exists).  A
+// subtree rooted at depth k, index x spans gaps [x S_k, (x+1) S_k - 1] with
+// S_k = (b+1)^(h-k).  lower/upper gap of sorted rank s:
+__device__ __forceinline__ void rank_gaps(const LearnedGeom &G, uint64_t s, uint64_t &lo, uint64_t &hi) {
+    const BtreeGeom &g = G.g;
+    if (s < g.l + g.i) {
+        uint64_t j, t;
+        G.fd.divmod(s, j, t);
+        lo = j;
+        hi = t < g.b ? j : j + 1;
+    } else if (s < g.lir) {
+        lo = hi = g.i;
+    } else {
+        lo = s - g.l - g.r;
+        hi = lo + 1;
+    }
+}
+
+template <typename K, int NV>
+__device__ __forceinline__ void node_scan(const K *__restrict__ A, uint64_t n, uint64_t i, K q, uint32_t &lt,
+                                          uint32_t &valid, bool &eq) {
+    constexpr int KPV = 16 / sizeof(K);
+    constexpr int B = NV * KPV;
+    lt = 0;
+    eq = false;
+    if (i + B <= n) {
+        valid = B;
+        const uint4 *node = reinterpret_cast<const uint4 *>(A + i);
+        uint4 v[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) v[j] = __ldg(node + j);
+        const K *all = reinterpret_cast<const K *>(v);
+#pragma unroll
+        for (int j = 0; j < B; ++j) lt += all[j] < q;
+        if (lt < (uint32_t)B) {
+            K at = all[0];
+#pragma unroll
+            for (int j = 1; j < B; ++j)
+                if ((uint32_t)j == lt) at = all[j];
+            eq = at == q;
+        }
+    } else {
+        valid = (uint32_t)(n - i);
+        for (uint32_t j = 0; j < valid; ++j) lt += __ldg(A + i + j) < q;
+        if (lt < valid) eq = __ldg(A + i + lt) == q;
+    }
+}
+
+template <typename K, int NV>
+__global__ void __launch_bounds__(256)
+learned_query_kernel(const K *__restrict__ A, const LearnedGeom G, const __grid_constant__ ModelParams p,
+                     int use_net, const tl_rank_leaf *__restrict__ leaves, const K *__restrict__ Q, uint64_t nq,
+                     uint64_t *__restrict__ ans, unsigned long long *__restrict__ stats) {
+    constexpr int B = NV * (16 / sizeof(K));
+    const BtreeGeom &g = G.g;
+    const uint64_t n = g.n;
+    const uint64_t cmax = (n + 1) / (B + 1);
+    unsigned long long n_fallback = 0, depth_sum = 0;
+    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
+         qi += (uint64_t)gridDim.x * blockDim.x) {
+        const K q = __ldcs(Q + qi);
+        uint64_t res = n;
+        bool done = false;
+        // 1. predicted rank window -> deepest covering subtree
+        const uint32_t l = leaf_of(p, root_eval(p, feature(p, (uint64_t)q), use_net != 0));
+        const tl_rank_leaf lf = leaves[l];
+        if (!lf.empty && g.h > 0) {
+            const uint64_t pr = leaf_predict(lf, (uint64_t)q, n);
+            const uint64_t rlo = pr > lf.eps_lo ? pr - lf.eps_lo : 0;
+            const uint64_t rhi = pr + lf.eps_hi < n ? pr + lf.eps_hi : n - 1;
+            uint64_t glo, ghi, t0, t1;
+            rank_gaps(G, rlo, glo, t0);
+            rank_gaps(G, rhi, t1, ghi);
+            uint32_t k = g.h;  // depth of the subtree root (h = a last-level node)
+            while (glo != ghi) {
+                glo = G.fd.div(glo);
+                ghi = G.fd.div(ghi);
+                --k;
+            }
+            // a last-level node that does not exist: start one level up
+            if (k == g.h && !(glo < g.i || (glo == g.i && g.r > 0))) {
+                glo = G.fd.div(glo);
+                --k;
+            }
+            depth_sum += k;
+            uint64_t i = g.pw[k] - 1 + glo * B;
+            bool less = false, greater = false;
+            while (i < n) {
+                uint32_t lt, valid;
+                bool eq;
+                node_scan<K, NV>(A, n, i, q, lt, valid, eq);
+                if (eq) {
+                    res = i + lt;
+                    done = true;
+                    break;
+                }
+                less |= lt > 0;
+                greater |= lt < valid;
+                if (i + 1 > cmax) break;
+                i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
+            }
+            if (!done && less && greater) done = true;  // absent: the subtree straddles q
+        }
+        // 2. plain search from the root when the window could not decide
+        if (!done) {
+            ++n_fallback;
+            uint64_t i = 0;
+            while (i < n) {
+                uint32_t lt, valid;
+                bool eq;
+                node_scan<K, NV>(A, n, i, q, lt, valid, eq);
+                if (eq) {
+                    res = i + lt;
+                    break;
+                }
+                if (i + 1 > cmax) break;
+                i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
+            }
+        }
+        __stcs(ans + qi, res);
+    }
+    if (stats) {
+        atomicAdd(&stats[0], n_fallback);
+        atomicAdd(&stats[1], depth_sum);
+    }
+}
+
+// ---------------------------------------------------------------- host
+static void init_model(tl_rank_model &m, const tl_rank_train_config &cfg) {
+    memset(&m, 0, sizeof m);
+    // layer 1: ramps with breakpoints spread over [0, 1]
+    for (int i = 0; i < H; ++i) {
+        m.w1[i] = 1.f;
+        m.b1[i] = -(float)i / H;
+    }
+    // layer 2: small deterministic pseudo-random weights
+    for (int j = 0; j < H; ++j) {
+        for (int i = 0; i < H; ++i) {
+            uint64_t r = mix64(cfg.seed * 1315423911ull + (uint64_t)(j * H + i));
+            m.w2[j][i] = ((float)(r >> 40) / (float)(1u << 24) - 0.5f) * (2.f / H);
+            if (cfg.monotone) m.w2[j][i] = fabsf(m.w2[j][i]);
+        }
+        m.b2[j] = 0.01f;
+        m.w3[j] = 1.f / H;
+    }
+    m.b3 = 0.f;
+}
+
+static void model_to_flat(const tl_rank_model &m, float *w) {
+    memcpy(w, m.w1, sizeof m.w1);
+    memcpy(w + H, m.b1, sizeof m.b1);
+    memcpy(w + 2 * H, m.w2, sizeof m.w2);
+    memcpy(w + 2 * H + H * H, m.b2, sizeof m.b2);
+    memcpy(w + 3 * H + H * H, m.w3, sizeof m.w3);
+    w[4 * H + H * H] = m.b3;
+}
+
+static void flat_to_model(const float *w, tl_rank_model &m) {
+    memcpy(m.w1, w, sizeof m.w1);
+    memcpy(m.b1, w + H, sizeof m.b1);
+    memcpy(m.w2, w + 2 * H, sizeof m.w2);
+    memcpy(m.b2, w + 2 * H + H * H, sizeof m.b2);
+    memcpy(m.w3, w + 3 * H + H * H, sizeof m.w3);
+    m.b3 = w[4 * H + H * H];
+}
+
+static int grid_for(uint64_t work, int threads) {
+    uint64_t g = (work + threads - 1) / threads;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 16));
+}
+
+static Feature feature_params(const tl_rank_model &m) {
+    Feature f;
+    f.x_lo = (float)m.x_lo;
+    f.x_scale = (float)m.x_scale;
+    f.log_feature = m.log_feature;
+    return f;
+}
+
+int rank_model_gradient(const tl_rank_model *m, const float *dx, const float *dy, uint32_t count, float *grad,
+                        float *loss, cudaStream_t st) {
+    if (!m || !dx || !dy || !grad || count == 0) return TL_ERROR_INVALID_VALUE;
+    const uint32_t blocks = (count + kTrainThreads - 1) / kTrainThreads;
+    float *buf = nullptr;
+    const size_t bytes = ((size_t)blocks * kParams + blocks + 2 * (kParams + 1)) * sizeof(float);
+    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&buf), bytes, st));
+    float *partial = buf, *lp = buf + (size_t)blocks * kParams, *g = lp + blocks, *w = g + kParams + 1;
+    float flat[kParams + 1] = {0};
+    model_to_flat(*m, flat);
+    cudaError_t e = cudaMemcpyAsync(w, flat, kParams * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        rmi_grad_kernel<<<blocks, kTrainThreads, 0, st>>>(w, feature_params(*m), dx, dy, nullptr, 1, 0, count,
+                                                          1.f / count, partial, lp);
+        rmi_reduce_kernel<<<8, 256, 0, st>>>(partial, lp, blocks, g, g + kParams);
+        e = cudaGetLastError();
+    }
+    float host[kParams + 1];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, g, sizeof host, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(buf, st);
+    if (e != cudaSuccess) {
+        record_cuda_error(e);
+        return TL_ERROR_CUDA;
+    }
+    memcpy(grad, host, kParams * sizeof(float));
+    if (loss) *loss = host[kParams];
+    return TL_SUCCESS;
+}
+
+int rank_model_train(const uint64_t *keys, uint64_t n, const tl_rank_train_config *cfg, tl_rank_model *out,
+                     tl_rank_leaf *leaves, cudaStream_t st) {
+    if (!keys || !cfg || !out || !leaves || n < 2) return TL_ERROR_INVALID_VALUE;
+    const uint32_t L = cfg->num_leaves;
+    if (L == 0 || (L & (L - 1)) || L > (1u << 24)) return TL_ERROR_INVALID_VALUE;
+    tl_rank_model m;
+    init_model(m, *cfg);
+    m.num_leaves = L;
+    m.log_feature = cfg->log_feature;
+    m.n = n;
+    uint64_t kfirst = 0, klast = 0;
+    TL_CUDA_TRY(cudaMemcpyAsync(&kfirst, keys, 8, cudaMemcpyDeviceToHost, st));
+    TL_CUDA_TRY(cudaMemcpyAsync(&klast, keys + n - 1, 8, cudaMemcpyDeviceToHost, st));
+    TL_CUDA_TRY(cudaStreamSynchronize(st));
+    const double f0 = m.log_feature ? (double)std::log2((float)kfirst + 1.0f) : (double)kfirst;
+    const double f1 = m.log_feature ? (double)std::log2((float)klast + 1.0f) : (double)klast;
+    m.x_lo = f0;
+    m.x_scale = f1 > f0 ? 1.0 / (f1 - f0) : 1.0;
+    const Feature fe = feature_params(m);
+
+    const uint32_t batch = std::max<uint32_t>(kTrainThreads, cfg->batch);
+    const uint32_t blocks = (batch + kTrainThreads - 1) / kTrainThreads;
+    float *buf = nullptr;
+    const size_t nfl = (size_t)blocks * kParams + blocks + 4 * (kParams + 1);
+    unsigned long long *ext = nullptr;
+    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&buf), nfl * sizeof(float), st));
+    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&ext), 4ull * L * sizeof(unsigned long long), st));
+    float *partial = buf, *lp = partial + (size_t)blocks * kParams, *grad = lp + blocks;
+    float *w = grad + kParams + 1, *mom = w + kParams + 1, *vel = mom + kParams + 1;
+    float flat[kParams + 1] = {0};
+    model_to_flat(m, flat);
+    TL_CUDA_TRY(cudaMemcpyAsync(w, flat, kParams * sizeof(float), cudaMemcpyHostToDevice, st));
+    TL_CUDA_TRY(cudaMemsetAsync(mom, 0, 2 * (kParams + 1) * sizeof(float), st));
+    const bool use_net = cfg->train_root != 0;
+    if (use_net) {
+        const float b1 = 0.9f, b2 = 0.999f;
+        float c1 = 1.f, c2 = 1.f;
+        for (uint32_t step = 0; step < cfg->steps; ++step) {
+            rmi_grad_kernel<<<blocks, kTrainThreads, 0, st>>>(w, fe, nullptr, nullptr, keys, n,
+                                                              mix64(cfg->seed + step), batch, 1.f / batch,
+                                                              partial, lp);
+            rmi_reduce_kernel<<<8, 256, 0, st>>>(partial, lp, blocks, grad, grad + kParams);
+            c1 *= b1;
+            c2 *= b2;
+            const float lr = cfg->lr * (step < cfg->steps / 2 ? 1.f : (step < 3 * cfg->steps / 4 ? 0.3f : 0.1f));
+            rmi_adam_kernel<<<8, 256, 0, st>>>(w, mom, vel, grad, lr, b1, b2, 1e-8f, 1.f - c1, 1.f - c2,
+                                               (int)cfg->monotone);
+            TL_CUDA_TRY(cudaGetLastError());
+        }
+        TL_CUDA_TRY(cudaMemcpyAsync(flat, w, kParams * sizeof(float), cudaMemcpyDeviceToHost, st));
+        TL_CUDA_TRY(cudaMemcpyAsync(&m.train_loss, grad + kParams, sizeof(float), cudaMemcpyDeviceToHost, st));
+        TL_CUDA_TRY(cudaStreamSynchronize(st));
+        flat_to_model(flat, m);
+    }
+    // leaves
+    const ModelParams p = to_params(m);
+    unsigned long long *kmin = ext, *kmax = ext + L, *rmin = ext + 2ull * L, *rmax = ext + 3ull * L;
+    TL_CUDA_TRY(cudaMemsetAsync(kmin, 0xFF, L * sizeof(unsigned long long), st));
+    TL_CUDA_TRY(cudaMemsetAsync(kmax, 0, L * sizeof(unsigned long long), st));
+    TL_CUDA_TRY(cudaMemsetAsync(rmin, 0xFF, L * sizeof(unsigned long long), st));
+    TL_CUDA_TRY(cudaMemsetAsync(rmax, 0, L * sizeof(unsigned long long), st));
+    const uint64_t chunks = (n + kLeafChunk - 1) / kLeafChunk;
+    leaf_extent_kernel<<<grid_for(chunks, 256), 256, 0, st>>>(p, use_net, keys, n, kmin, kmax, rmin, rmax);
+    leaf_fit_kernel<<<grid_for(L, 256), 256, 0, st>>>(L, kmin, kmax, rmin, rmax, leaves);
+    leaf_eps_kernel<<<grid_for(chunks, 256), 256, 0, st>>>(p, use_net, keys, n, leaves);
+    TL_CUDA_TRY(cudaGetLastError());
+    cudaFreeAsync(buf, st);
+    cudaFreeAsync(ext, st);
+    TL_CUDA_TRY(cudaStreamSynchronize(st));
+    m.train_root = use_net ? 1 : 0;
+    *out = m;
+    return TL_SUCCESS;
+}
+
+int rank_model_predict(const tl_rank_model *m, const tl_rank_leaf *leaves, const uint64_t *keys, uint64_t q,
+                       uint64_t *rank, uint32_t *eps, cudaStream_t st) {
+    if (!m || !leaves || (q && (!keys || !rank))) return TL_ERROR_INVALID_VALUE;
+    if (q == 0) return TL_SUCCESS;
+    rmi_predict_kernel<<<grid_for(q, 256), 256, 0, st>>>(to_params(*m), m->train_root != 0, leaves, keys, q, m->n,
+                                                         rank, eps);
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
+int query_btree_learned(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank_model *m,
+                        const tl_rank_leaf *leaves, const uint64_t *Q, uint64_t q, uint64_t *ans,
+                        unsigned long long *stats, cudaStream_t st, float *ms) {
+    if (!m || !leaves || (q && (!Q || !ans)) || (n && !A)) return TL_ERROR_INVALID_VALUE;
+    if (m->n != n) return TL_ERROR_INVALID_VALUE;
+    if (b * 8 % 16 || b * 8 > 256) return TL_ERROR_UNSUPPORTED;  // vector node loads: b in {2,4,8,16,32}
+    if (q == 0) return TL_SUCCESS;
+    LearnedGeom G;
+    G.g = make_btree_geom(n, b);
+    G.fd = FastDiv64(b + 1);
+    EventTimer timer(ms != nullptr, st);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    timer.start();
+    const ModelParams p = to_params(*m);
+    const int use_net = m->train_root != 0;
+    auto launch = [&](auto kern) -> int {
+        int per_sm = 0;
+        TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+        uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, (q + 255) / 256);
+        kern<<<(unsigned)std::max<uint64_t>(grid, 1), 256, 0, st>>>(A, G, p, use_net, leaves, Q, q, ans, stats);
+        return TL_SUCCESS;
+    };
+    int rc;
+    switch (b * 8 / 16) {
+        case 1: rc = launch(learned_query_kernel<uint64_t, 1>); break;
+        case 2: rc = launch(learned_query_kernel<uint64_t, 2>); break;
+        case 4: rc = launch(learned_query_kernel<uint64_t, 4>); break;
+        case 8: rc = launch(learned_query_kernel<uint64_t, 8>); break;
+        case 16: rc = launch(learned_query_kernel<uint64_t, 16>); break;
+        default: return TL_ERROR_UNSUPPORTED;
+    }
+    if (rc) return rc;
+    timer.stop();
+    TL_CUDA_TRY(cudaGetLastError());
+    if (ms) {
+        rc = sync_and_check(st);
+        if (rc) return rc;
+        *ms = timer.elapsed();
+    }
+    return TL_SUCCESS;
+}
+
+}  // namespace tl

@@ -23,6 +23,7 @@
 #include <mutex>
 #include <vector>
 
+#include "btree_plan.cuh"
 #include "geometry.cuh"
 #include "internal.h"
 #include "stream.cuh"
@@ -30,7 +31,6 @@
 namespace tl {
 
 constexpr int kStreamThreads = 256;
-constexpr int kScatterThreads = 256;
 constexpr uint32_t kUnitMaxLevels = 8;
 
 template <typename K>
@@ -40,149 +40,10 @@ constexpr uint64_t stream_tile_keys() {
 
 static inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
-// ---------------------------------------------------------------- B-tree stream
-// Two schedules.  Plan R (right to left): the last level's keys go straight to
-// their final positions (they move right), the whole top tree goes through
-// scratch.  Plan L (left to right), for trees whose top tree holds most keys:
-// the top tree's own last level goes straight to its final positions (those
-// keys move left), the last level and the upper top levels go through scratch.
-// The host picks the plan with the smaller scratch (the second pass's traffic).
-enum BtreePlan { PLAN_R = 0, PLAN_L = 1 };
-
-struct BtreeStream {
-    BtreeGeom g;
-    FastDiv64 fd;
-    uint64_t tile_keys, ntiles;
-    int plan;
-    uint64_t i2;          // plan L: first position of the top tree's last level, (b+1)^(h-1) - 1
-    uint64_t ibase;       // plan L: floor(i / (b+1))
-    uint64_t nscratch;    // scratch slots
-};
-
-TL_HD uint64_t btree_tile_of_ticket(const BtreeStream &S, uint64_t t) {
-    return S.plan == PLAN_R ? S.ntiles - 1 - t : t;
-}
-
-// Source range of tile k (tiles ascend with position).
-TL_HD void btree_tile(const BtreeStream &S, uint64_t k, uint64_t &p0, uint64_t &p1) {
-    p0 = k * S.tile_keys;
-    p1 = p0 + S.tile_keys < S.g.n ? p0 + S.tile_keys : S.g.n;
-}
-
-// Plan R: sorted rank -> destination of a last-level key, extended monotonically
-// over the separators in between; bounds the destinations of a tile.
-TL_HD uint64_t btree_leaf_dest_bound(const BtreeStream &S, uint64_t s) {
-    return s < S.g.l + S.g.i ? S.g.ni + s - S.fd.div(s) : S.g.ni + s - S.g.i;
-}
-
-// Plan L: sorted rank s >= lir (top rank c) -> destination of a key of the top
-// tree's last level, extended monotonically over the upper keys.
-TL_HD uint64_t btree_top_last_dest_bound(const BtreeStream &S, uint64_t s) {
-    const uint64_t c = s - S.g.l - S.g.r;
-    return S.i2 + c - S.fd.div(c + 1);
-}
-
-// Tiles (other than k) whose source lies under the direct destinations of tile
-// [p0, p1): right of the tile for plan R, left of it for plan L, i.e. always
-// tiles with earlier tickets.  False if there are none.
-TL_HD bool btree_tile_wait(const BtreeStream &S, uint64_t p0, uint64_t p1, uint64_t &k_lo, uint64_t &k_hi) {
-    const BtreeGeom &g = S.g;
-    if (S.plan == PLAN_R) {
-        if (p0 >= g.lir) return false;
-        uint64_t d0 = btree_leaf_dest_bound(S, p0);
-        uint64_t d1 = btree_leaf_dest_bound(S, (p1 < g.lir ? p1 : g.lir) - 1) + 1;
-        if (d1 > g.n) d1 = g.n;  // a trailing separator bounds past the last leaf key
-        uint64_t lo = d0 > p1 ? d0 : p1;
-        if (lo >= d1) return false;
-        k_lo = lo / S.tile_keys;
-        k_hi = (d1 - 1) / S.tile_keys;
-        return true;
-    }
-    if (p1 <= g.lir) return false;
-    uint64_t d0 = btree_top_last_dest_bound(S, p0 > g.lir ? p0 : g.lir);
-    uint64_t d1 = btree_top_last_dest_bound(S, p1 - 1) + 1;
-    uint64_t hi = d1 < p0 ? d1 : p0;
-    if (d0 >= hi) return false;
-    k_lo = d0 / S.tile_keys;
-    k_hi = (hi - 1) / S.tile_keys;
-    return true;
-}
-
-// Where sorted rank x goes in the stream pass: true -> A[idx] (final position),
-// false -> scratch[idx].
-TL_HD bool btree_place(const BtreeStream &S, uint64_t x, uint64_t &idx) {
-    const BtreeGeom &g = S.g;
-    if (S.plan == PLAN_L) {
-        if (x < g.lir) {
-            idx = x;
-            return false;
-        }
-        const uint64_t c = x - g.l - g.r;
-        uint64_t q, rem;
-        S.fd.divmod(c + 1, q, rem);
-        if (rem != 0) {
-            idx = S.i2 + c - q;
-            return true;
-        }
-        idx = g.lir + q - 1 - S.ibase;
-        return false;
-    }
-    if (x < g.l + g.i) {
-        uint64_t j, t;
-        S.fd.divmod(x, j, t);
-        if (t < g.b) {
-            idx = g.ni + j * g.b + t;
-            return true;
-        }
-        idx = j;
-        return false;
-    }
-    if (x < g.lir) {
-        idx = g.ni + x - g.i;
-        return true;
-    }
-    idx = x - g.l - g.r;
-    return false;
-}
-
-// Final position of the key held by scratch slot `slot`.
-TL_HD uint64_t btree_slot_dest(const BtreeStream &S, uint64_t slot) {
-    const BtreeGeom &g = S.g;
-    if (S.plan == PLAN_R) return btree_perfect_pos(g, S.fd, slot, g.h);
-    uint64_t s;
-    if (slot < g.lir) {
-        s = slot;
-    } else {
-        const uint64_t M = slot - g.lir + S.ibase + 1;
-        s = M * (g.b + 1) - 1 + g.l + g.r;
-    }
-    return btree_pos(g, S.fd, s);
-}
-
-__host__ inline void btree_choose_plan(BtreeStream &S) {
-    const BtreeGeom &g = S.g;
-    S.plan = PLAN_R;
-    S.nscratch = g.ni;
-    if (g.h < 1) return;
-    const uint64_t i2 = g.pw[g.h - 1] - 1;
-    const uint64_t ibase = g.i / (g.b + 1);
-    // Plan L needs every direct key to move left: i2 <= l + r + floor((c+1)/(b+1))
-    // at the smallest trailing top rank c = i.
-    if (g.lir >= g.n) return;
-    if (i2 > g.l + g.r + (g.i + 1) / (g.b + 1)) return;
-    const uint64_t upper = g.ni / (g.b + 1) - ibase;
-    const uint64_t nscr = g.lir + upper;
-    if (nscr < g.ni) {
-        S.plan = PLAN_L;
-        S.i2 = i2;
-        S.ibase = ibase;
-        S.nscratch = nscr;
-    }
-}
-
 template <typename K>
 __global__ void __launch_bounds__(kStreamThreads)
-btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl *ctrl, unsigned int *flags) {
+btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl *ctrl, WaitCfg wc,
+                    unsigned int *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sm = reinterpret_cast<K *>(smem_raw);
     __shared__ unsigned long long s_ticket;
@@ -190,32 +51,16 @@ btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl 
     for (;;) {
         unsigned long long t = next_ticket(ctrl, &s_ticket);
         if (t >= S.ntiles) break;
-        const uint64_t k = btree_tile_of_ticket(S, t);
-        uint64_t p0, p1;
-        btree_tile(S, k, p0, p1);
-        const uint64_t base = load_tile(A, p0, p1, sm);
-        publish_read(&flags[k], ctrl);
-        uint64_t k_lo, k_hi;
-        if (btree_tile_wait(S, p0, p1, k_lo, k_hi) &&
-            !wait_tiles(flags, (long long)k_lo, (long long)k_hi, ctrl, &s_ok))
-            continue;
-        for (uint64_t x = p0 + threadIdx.x; x < p1; x += blockDim.x) {
-            uint64_t idx;
-            const K key = sm[x - base];
-            if (btree_place(S, x, idx))
-                A[idx] = key;
-            else
-                scr[idx] = key;
-        }
+        btree_stream_tile(S, A, scr, flags, ctrl, wc, btree_tile_of_ticket(S, t), sm, &s_ok);
     }
 }
 
 template <typename K>
 __global__ void __launch_bounds__(kScatterThreads)
 btree_scatter_kernel(K *__restrict__ A, const K *__restrict__ scr, BtreeStream S) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < S.nscratch; c += stride)
-        A[btree_slot_dest(S, c)] = __ldcs(scr + c);
+    for (uint64_t c0 = (uint64_t)blockIdx.x * kScatterChunk; c0 < S.nscratch;
+         c0 += (uint64_t)gridDim.x * kScatterChunk)
+        btree_scatter_chunk(S, A, scr, c0);
 }
 
 // ---------------------------------------------------------------- mvEB stream
@@ -280,7 +125,7 @@ TL_HD uint64_t mveb_slot_rank(const MvebPlan &P, uint64_t s) {
 template <typename K>
 __global__ void __launch_bounds__(kStreamThreads)
 mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant__ MvebParams prm,
-                   Ctrl *ctrl, unsigned int *flags) {
+                   Ctrl *ctrl, WaitCfg wc, unsigned int *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sm = reinterpret_cast<K *>(smem_raw);
     __shared__ unsigned long long s_ticket;
@@ -303,7 +148,7 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
             loaded_U = R.U;
         }
         const uint64_t base = load_tile(A, p0, p1, sm);
-        publish_read(&flags[k], ctrl);
+        publish_read(&flags[k], wc);
         if (R.U == 0) {
             for (uint64_t x = p0 + threadIdx.x; x < p1; x += blockDim.x)
                 scr[R.slot_base + (x - R.src)] = sm[x - base];
@@ -311,7 +156,7 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
         }
         uint64_t k_lo, k_hi;
         if (mveb_tile_wait(P, R, p0, p1, k_lo, k_hi) &&
-            !wait_tiles(flags, (long long)k_lo, (long long)k_hi, ctrl, &s_ok))
+            !wait_tiles(flags, (long long)k_lo, (long long)k_hi, ctrl, wc, &s_ok))
             continue;
         const uint32_t U = R.U;
         const uint64_t u = (1ull << U) - 1;
@@ -332,7 +177,18 @@ __global__ void __launch_bounds__(kScatterThreads)
 mveb_scatter_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_constant__ MvebParams prm) {
     const MvebPlan &P = prm.plan;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < P.total_slots; s += stride) {
+    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; s + 3 * stride < P.total_slots; s += 4 * stride) {
+        K v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = __ldcs(scr + s + u * stride);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t rank = mveb_slot_rank(P, s + u * stride);
+            if (rank != ~0ull) A[mveb_pos(P.n, rank)] = v[u];
+        }
+    }
+    for (; s < P.total_slots; s += stride) {
         const uint64_t rank = mveb_slot_rank(P, s);
         if (rank != ~0ull) A[mveb_pos(P.n, rank)] = scr[s];
     }
@@ -380,6 +236,7 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
         if (b >= (1ull << 31)) return TL_ERROR_UNSUPPORTED;
         pl.bs.g = make_btree_geom(n, b);
         pl.bs.fd = FastDiv64(b + 1);
+        pl.bs.fd32 = FastDiv32((uint32_t)(b + 1));
         pl.bs.tile_keys = pl.tile_keys;
         pl.ntiles = (n + pl.tile_keys - 1) / pl.tile_keys;
         pl.bs.ntiles = pl.ntiles;
@@ -409,13 +266,12 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
     K *scr = reinterpret_cast<K *>(ws);
     unsigned int *flags = reinterpret_cast<unsigned int *>(ws + pl.off_flags);
     Ctrl *ctrl = reinterpret_cast<Ctrl *>(ws + pl.off_ctrl);
-    Ctrl h{};
-    h.flag_value = 1;
-    h.wait_value = debug_force_timeout() ? 0xFFFFFFFFu : 1u;  // forced: no tile ever publishes it
-    h.spin_limit = debug_spin_limit();
-    // Clear the flags, then set up the control block; both stream-ordered.
-    if (pl.ntiles) TL_CUDA_TRY(cudaMemsetAsync(flags, 0, pl.ntiles * sizeof(unsigned int), st));
-    TL_CUDA_TRY(cudaMemcpyAsync(ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    WaitCfg wc;
+    wc.flag_value = 1;
+    wc.wait_value = debug_force_timeout() ? 0xFFFFFFFFu : 1u;  // forced: no tile ever publishes it
+    wc.spin_limit = debug_spin_limit();
+    // flags and control block are contiguous: one stream-ordered memset clears both
+    TL_CUDA_TRY(cudaMemsetAsync(flags, 0, pl.bytes - pl.off_flags, st));
     const size_t smem = (size_t)pl.tile_keys * sizeof(K) + 16;
     const int smx = sm_count();
     if (pl.layout == TL_LAYOUT_MVEB) {
@@ -424,7 +280,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         int per_sm = 0;
         TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
         uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * smx, std::max<uint64_t>(pl.ntiles, 1));
-        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.mp, ctrl, flags);
+        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.mp, ctrl, wc, flags);
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
         if (pl.scratch_keys) {
@@ -439,11 +295,11 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         int per_sm = 0;
         TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
         uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * smx, std::max<uint64_t>(pl.ntiles, 1));
-        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, flags);
+        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, wc, flags);
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
         if (pl.scratch_keys) {
-            uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterThreads - 1) / kScatterThreads,
+            uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterChunk - 1) / kScatterChunk,
                                              (uint64_t)smx * 8);
             btree_scatter_kernel<K><<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.bs);
             TL_CUDA_TRY(cudaGetLastError());
@@ -574,9 +430,15 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
                 ++slot_writes[s];
             };
             if (!mv) {
+                const TileDiv td = btree_tile_div(pl.bs, p0);
+                const Regime RG = btree_stream_regime(pl.bs, p0, p1);
                 for (uint64_t x = p0; x < p1; ++x) {
-                    uint64_t idx;
-                    if (btree_place(pl.bs, x, idx)) W(idx, tile[x - p0]); else SC(idx, tile[x - p0]);
+                    uint64_t idx, idx2, idx3;
+                    const bool direct = btree_place_tile(pl.bs, td, x, idx);
+                    if (direct != btree_place(pl.bs, x, idx2) || idx != idx2) ++viol;  // fast path == reference form
+                    if (RG.kind && (btree_regime_place(pl.bs, RG, (uint32_t)(x - p0), idx3) != direct || idx3 != idx))
+                        ++viol;
+                    if (direct) W(idx, tile[x - p0]); else SC(idx, tile[x - p0]);
                 }
             } else {
                 const MvebRegion &R = P.reg[ri];
@@ -603,7 +465,16 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
         if (!mv) {
             for (uint64_t c = 0; c < pl.bs.nscratch; ++c) {
                 if (slot_writes[c] != 1) ++viol;
+                const uint64_t cc0 = c - c % kScatterChunk;
+                const ScatterDiv sd = btree_scatter_div(pl.bs, cc0);
                 const uint64_t d = btree_slot_dest(pl.bs, c);
+                if (btree_slot_dest_tile(pl.bs, sd, c) != d) ++viol;  // fast path == reference form
+                const Regime RG = btree_scatter_regime(pl.bs, cc0, std::min(pl.bs.nscratch, cc0 + kScatterChunk));
+                if (RG.kind == 1) {
+                    const uint32_t vv = RG.r0 + (uint32_t)(c - cc0);
+                    const uint32_t ql = pl.bs.fd32.div(vv);
+                    if (vv - ql * pl.bs.fd32.d != RG.skip && RG.dbase + (vv - ql) != d) ++viol;
+                }
                 if (d >= n) { ++viol; continue; }
                 A[d] = scr[c];
                 ++pos_writes[d];

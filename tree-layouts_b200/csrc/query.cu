@@ -119,6 +119,66 @@ btree_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_t P, 
     }
 }
 
+// One thread per query, for nodes of b*w = 16*NV bytes (node starts are then
+// 16-byte aligned): the node is fetched with NV independent 16-byte loads, so a
+// warp keeps 32 descents in flight.  The last, partially filled leaf (the only
+// node that may cross n) is read with guarded scalar loads.
+template <typename K, int NV>
+__global__ void __launch_bounds__(kQueryThreads)
+btree_query_vec_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, const K *__restrict__ Q, uint64_t nq,
+                       uint64_t *__restrict__ ans) {
+    constexpr int KPV = 16 / sizeof(K);  // keys per 16-byte vector
+    constexpr int B = NV * KPV;          // == b
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t cmax = (n + 1) / (B + 1);
+    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
+        const K q = __ldcs(Q + qi);
+        uint64_t i = 0, res = n;
+        while (i < n) {
+            uint32_t lt = 0;
+            bool eq = false;
+            if (i + B <= n) {
+                const uint4 *node = reinterpret_cast<const uint4 *>(A + i);
+                uint4 v[NV];
+#pragma unroll
+                for (int j = 0; j < NV; ++j) v[j] = __ldg(node + j);
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+                    const K *kk = reinterpret_cast<const K *>(&v[j]);
+#pragma unroll
+                    for (int e = 0; e < KPV; ++e) lt += kk[e] < q;
+                }
+                if (lt < (uint32_t)B) {
+                    const K *all = reinterpret_cast<const K *>(v);
+                    K at = all[0];
+#pragma unroll
+                    for (int j = 1; j < B; ++j)
+                        if ((uint32_t)j == lt) at = all[j];
+                    eq = at == q;
+                }
+            } else {
+                const uint64_t valid = n - i;
+                K at = q;
+                for (uint64_t j = 0; j < valid; ++j) {
+                    const K cur = __ldg(A + i + j);
+                    lt += cur < q;
+                }
+                if (lt < valid) {
+                    at = __ldg(A + i + lt);
+                    eq = at == q;
+                }
+            }
+            if (eq) {
+                res = i + lt;
+                break;
+            }
+            if (i + 1 > cmax) break;
+            i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
+        }
+        __stcs(ans + qi, res);
+    }
+}
+
 // ---------------------------------------------------------------- mvEB
 // searchvEB (gpu/src/query-mveb.cuh:43-66): BFS index i and the table recurrence
 // pos[d] = pos[D_d] + R_d + (i & R_d) * L_d, with pos[] in shared memory, one
@@ -246,6 +306,29 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
         }
         P = std::min<uint64_t>(top, a.n);
         size_t smem = P * sizeof(K);
+        const uint64_t node_bytes = a.b * sizeof(K);
+        const int nv = (node_bytes % 16 == 0 && node_bytes <= 256) ? (int)(node_bytes / 16) : 0;
+        if (nv == 1 || nv == 2 || nv == 4 || nv == 8 || nv == 16) {
+            int rc = TL_SUCCESS;
+#define TL_BV(NV)                                                                          \
+    case NV: {                                                                             \
+        auto kern = btree_query_vec_kernel<K, NV>;                                         \
+        rc = persistent_grid(kern, 0, a.q, &grid);                                         \
+        if (rc) return rc;                                                                 \
+        kern<<<grid, kQueryThreads, 0, st>>>(A, a.n, a.b, Q, a.q, a.answers);              \
+        break;                                                                             \
+    }
+            switch (nv) {
+                TL_BV(1)
+                TL_BV(2)
+                TL_BV(4)
+                TL_BV(8)
+                TL_BV(16)
+            }
+#undef TL_BV
+            TL_CUDA_TRY(cudaGetLastError());
+            return TL_SUCCESS;
+        }
         int G = 1;
         while (G < 32 && (uint64_t)G < a.b) G <<= 1;
         int rc = TL_SUCCESS;

@@ -16,13 +16,19 @@
 
 namespace tl {
 
+// Per-launch control block in device memory: zeroed (one memset) before each
+// launch, so a launch needs no host-to-device copy and can be captured in a graph.
 struct Ctrl {
     unsigned long long ticket;
     unsigned int error;
-    unsigned int flag_value;      // value a tile publishes once its source is read
-    unsigned int wait_value;      // value a wait expects (== flag_value except in fault tests)
-    unsigned int spin_limit;      // iterations of a bounded wait (x ~256 ns each)
-    unsigned int pad[10];
+    unsigned int pad[13];
+};
+
+// Wait parameters, passed to the kernels by value.
+struct WaitCfg {
+    unsigned int flag_value;  // value a tile publishes once its source is read
+    unsigned int wait_value;  // value a wait expects (== flag_value except in fault tests)
+    unsigned int spin_limit;  // iterations of a bounded wait (x ~256 ns each)
 };
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
@@ -36,8 +42,9 @@ __device__ __forceinline__ void st_release(unsigned int *p, unsigned int v) {
 }
 
 // Waits until flag == want; false (and the error recorded) if the bound expires.
-__device__ __forceinline__ bool wait_flag(const unsigned int *flag, unsigned int want, Ctrl *ctrl) {
-    unsigned int limit = ctrl->spin_limit;
+__device__ __forceinline__ bool wait_flag(const unsigned int *flag, unsigned int want, Ctrl *ctrl,
+                                          const WaitCfg &wc) {
+    unsigned int limit = wc.spin_limit;
     unsigned int ns = 32;
     for (unsigned int it = 0; it <= limit; ++it) {
         if (ld_acquire(flag) == want) return true;
@@ -57,29 +64,31 @@ __device__ __forceinline__ unsigned long long next_ticket(Ctrl *ctrl, unsigned l
 }
 
 // Block-wide: publish that this tile's source has been read into shared memory.
-__device__ __forceinline__ void publish_read(unsigned int *flag, Ctrl *ctrl) {
+__device__ __forceinline__ void publish_read(unsigned int *flag, const WaitCfg &wc) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        st_release(flag, ctrl->flag_value);
+        st_release(flag, wc.flag_value);
     }
 }
 
 // Block-wide: wait for tiles [k_lo, k_hi] (inclusive, global tile ids) to be read.
 // Returns true when all were seen before the bound expired.
 __device__ __forceinline__ bool wait_tiles(const unsigned int *flags, long long k_lo, long long k_hi,
-                                           Ctrl *ctrl, int *s_ok) {
+                                           Ctrl *ctrl, const WaitCfg &wc, int *s_ok) {
     if (threadIdx.x == 0) *s_ok = 1;
     __syncthreads();
     for (long long k = k_lo + threadIdx.x; k <= k_hi; k += blockDim.x)
-        if (!wait_flag(&flags[k], ctrl->wait_value, ctrl)) *s_ok = 0;
+        if (!wait_flag(&flags[k], wc.wait_value, ctrl, wc)) *s_ok = 0;
     __syncthreads();
     return *s_ok != 0;
 }
 
 // Copies src[p0, p1) into shared memory so that element x sits at
 // sm[x - base], base = p0 rounded down to a 16-byte boundary of the global
-// address.  Returns base.  Interior 16-byte chunks use vector loads.
+// address.  Returns base when the copy has landed.  The 16-byte-aligned interior
+// goes through cp.async (global -> shared without registers), so every thread
+// has all of its copies in flight at once; the ragged ends use plain loads.
 template <typename K>
 __device__ __forceinline__ uint64_t load_tile(const K *__restrict__ src, uint64_t p0, uint64_t p1, K *sm) {
     constexpr uint32_t V = 16 / sizeof(K);
@@ -91,10 +100,14 @@ __device__ __forceinline__ uint64_t load_tile(const K *__restrict__ src, uint64_
     uint64_t nvec = (p1 - a0) / V;
     uint64_t a1 = a0 + nvec * V;
     for (uint64_t x = p0 + threadIdx.x; x < a0; x += blockDim.x) sm[x - base] = src[x];
-    const uint4 *vsrc = reinterpret_cast<const uint4 *>(src + a0);
-    uint4 *vdst = reinterpret_cast<uint4 *>(sm + (a0 - base));
-    for (uint64_t v = threadIdx.x; v < nvec; v += blockDim.x) vdst[v] = __ldcs(vsrc + v);
+    const char *gsrc = reinterpret_cast<const char *>(src + a0);
+    const uint32_t sdst = (uint32_t)__cvta_generic_to_shared(sm + (a0 - base));
+    for (uint64_t v = threadIdx.x; v < nvec; v += blockDim.x)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst + (uint32_t)(v * 16)),
+                     "l"(gsrc + v * 16)
+                     : "memory");
     for (uint64_t x = a1 + threadIdx.x; x < p1; x += blockDim.x) sm[x - base] = src[x];
+    asm volatile("cp.async.wait_all;" ::: "memory");
     return base;
 }
 

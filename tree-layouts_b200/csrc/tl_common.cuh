@@ -42,6 +42,26 @@ struct FastDiv64 {
     }
 };
 
+// floor(x / d) for 32-bit x and an invariant divisor 2 <= d < 2^31 (same method).
+struct FastDiv32 {
+    uint32_t d = 2, m = 0, sh = 0;
+    FastDiv32() = default;
+    __host__ explicit FastDiv32(uint32_t div) : d(div) {
+        uint32_t l = 0;
+        while (l < 32 && (1ull << l) < div) ++l;
+        m = (uint32_t)((((1ull << l) - div) << 32) / div + 1);
+        sh = l - 1;
+    }
+    TL_HD uint32_t div(uint32_t x) const {
+#ifdef __CUDA_ARCH__
+        uint32_t t = __umulhi(m, x);
+#else
+        uint32_t t = (uint32_t)(((uint64_t)m * x) >> 32);
+#endif
+        return (t + ((x - t) >> 1)) >> sh;
+    }
+};
+
 TL_HD uint32_t bit_length(uint64_t x) {
 #ifdef __CUDA_ARCH__
     return 64u - (uint32_t)__clzll((long long)x);

@@ -81,3 +81,101 @@ def queries_torch(keys, q: int, hit_frac: float, seed: int, lo: int | None = Non
 
 def _as_unsigned(v: int, nbytes: int) -> int:
     return v & ((1 << (8 * nbytes)) - 1)
+
+
+# ------------------------------------------------------------------ skewed keys, Zipf queries
+def skewed_keys_torch(n: int, seed: int, device="cuda", oversample: float = 1.08):
+    """n unique sorted keys (int64 tensor, values in [0, 2^62]): the sorted,
+    deduplicated union of (a) lognormal(mu=0, sigma=2) samples scaled into
+    [0, 2^62] (x / e^12 * 2^62, clamped: e^12 is the +6 sigma point) and
+    (b) 5% of the keys from 1000 clusters with uniform centres and width 2^20;
+    thinned evenly to exactly n."""
+    import math
+
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    n_a = int(n * 0.95 * oversample)
+    n_b = int(n * 0.05 * oversample)
+    z = torch.randn(n_a, generator=g, device=device, dtype=torch.float64)
+    z.mul_(2.0).exp_().div_(math.exp(12.0)).clamp_(max=1.0).mul_(float(2**62))
+    a = z.to(torch.int64)
+    del z
+    centres = torch.randint(0, 2**62 - 2**20, (1000,), generator=g, device=device, dtype=torch.int64)
+    cid = torch.randint(0, 1000, (n_b,), generator=g, device=device, dtype=torch.int64)
+    bk = centres[cid] + torch.randint(0, 2**20, (n_b,), generator=g, device=device, dtype=torch.int64)
+    del cid
+    allk = torch.unique(torch.cat([a, bk]))
+    del a, bk
+    m = allk.numel()
+    if m < n:
+        raise RuntimeError(f"only {m} unique keys for n={n}; raise oversample")
+    idx = torch.arange(n, device=device, dtype=torch.int64).mul_(m).div_(n, rounding_mode="floor")
+    return allk[idx]
+
+
+def zipf_queries_torch(keys, q: int, seed: int, s: float = 1.1, hit_frac: float = 0.9):
+    """hit_frac of the queries are keys whose popularity rank follows Zipf(s)
+    (inverse CDF of the continuous power law on [1, n+1)), popularity rank k
+    mapped to key index (k * 2654435761) mod n so that popular keys spread over
+    the key space; the rest are uniform values in [min key, max key]."""
+    import torch
+    dev = keys.device
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    n = keys.numel()
+    nh = int(round(q * hit_frac))
+    u = torch.rand(nh, generator=g, device=dev, dtype=torch.float64)
+    a = 1.0 - s
+    k = (((float(n + 1) ** a - 1.0) * u + 1.0) ** (1.0 / a)).floor_().clamp_(1, n).to(torch.int64) - 1
+    ranks = (k * 2654435761) % n
+    hits = keys[ranks]
+    lo, hi = int(keys[0].item()), int(keys[-1].item())
+    miss = torch.randint(0, 2**62, (q - nh,), generator=g, device=dev, dtype=torch.int64) % (hi - lo + 1) + lo
+    out = torch.cat([hits, miss])
+    return out[torch.randperm(q, generator=g, device=dev)]
+
+
+# ------------------------------------------------------------------ batched workload
+def batch_keys_torch(sizes, gap_hi: int, seed: int, device="cuda"):
+    """Concatenated sorted instances (each: prefix sums of uniform gaps in
+    [1, gap_hi], its own seed-derived stream) and the int64 offset table."""
+    import numpy as np
+    import torch
+    sizes = np.asarray(sizes, dtype=np.int64)
+    offsets = np.zeros(len(sizes) + 1, dtype=np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    total = int(offsets[-1])
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    gaps = torch.randint(1, gap_hi + 1, (total,), generator=g, device=device, dtype=torch.int64)
+    keys = torch.cumsum(gaps, 0)
+    off_t = torch.from_numpy(offsets).to(device)
+    # restart every instance's prefix sum at its own first gap
+    starts = off_t[:-1]
+    base = torch.zeros(len(sizes), dtype=torch.int64, device=device)
+    nz = starts > 0
+    base[nz] = keys[starts[nz] - 1]
+    keys -= torch.repeat_interleave(base, torch.from_numpy(sizes).to(device))
+    return keys, off_t
+
+
+def batch_queries_torch(keys, offsets, q: int, hit_frac: float, seed: int):
+    """q queries, each tagged with a uniform instance id: hit_frac drawn from that
+    instance's keys, the rest uniform in its [min, max]."""
+    import torch
+    dev = keys.device
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    num = offsets.numel() - 1
+    inst = torch.randint(0, num, (q,), generator=g, device=dev, dtype=torch.int64)
+    lo_i, hi_i = offsets[inst], offsets[inst + 1]
+    size = hi_i - lo_i
+    u = torch.rand(q, generator=g, device=dev, dtype=torch.float64)
+    pos = lo_i + (u * size.double()).long().clamp_max(size - 1)
+    hits = keys[pos]
+    kmin, kmax = keys[lo_i], keys[hi_i - 1]
+    r = torch.randint(0, 2**62, (q,), generator=g, device=dev, dtype=torch.int64)
+    miss = kmin + r % (kmax - kmin + 1)
+    is_hit = torch.rand(q, generator=g, device=dev) < hit_frac
+    return torch.where(is_hit, hits, miss), inst.to(torch.int32)
