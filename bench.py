@@ -38,6 +38,9 @@ WORKLOADS = {
     "mveb-n300M-u32": ("mveb", 0, 300_000_000, 4, 3, 5, 2**27, 6),
     "bst-n2^30-1-u64": ("bst", 1, 2**30 - 1, 8, 16, 1, 2**27, 2),
     "bst-n2^20-1-u64": ("bst", 1, 2**20 - 1, 8, 16, 1, 2**20, 2),
+    # small cases for ncu captures (inputs above L2, a few GB on the device)
+    "btree-b8-n60M-u64": ("btree", 8, 60_000_000, 8, 16, 3, 2**24, 4),
+    "bst-n2^26-1-u64": ("bst", 1, 2**26 - 1, 8, 16, 1, 2**24, 2),
 }
 DEFAULT = "btree-b16-n500M-u64"
 METRIC = "permute GB/s (2*n*key_bytes / device time), in-place sorted -> level-order B-tree"
@@ -176,7 +179,7 @@ def run_reference(args, rank):
         print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU code has no mvEB layout "
                           "(cpu/src builds the standard vEB); its mvEB exists only as GPU code"}))
         return
-    n_sample = min(n, args.cpu_sample)
+    n_sample = min(n, args.ref_n) if args.ref_n else n
     steps = []
     for _ in range(args.warmup):
         cpu_reference_permute(layout, b, n_sample, kb, 1, 0)
@@ -287,9 +290,10 @@ def batched_section(args, dev):
     for i in range(args.warmup + args.steps):
         keys.copy_(pristine)
         torch.cuda.synchronize()
-        e0.record(s)
-        g.replay()
-        e1.record(s)
+        with torch.cuda.stream(s):  # CUDAGraph.replay launches on the current stream
+            e0.record(s)
+            g.replay()
+            e1.record(s)
         torch.cuda.synchronize()
         if i >= args.warmup:
             ms.append(e0.elapsed_time(e1))
@@ -480,6 +484,7 @@ def main():
     ap.add_argument("--queries", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=50_000_000)
+    ap.add_argument("--ref-n", type=int, default=0, help="reference arm keys (0: the workload's full n)")
     ap.add_argument("--learned", type=int, default=1, help="learned-vs-plain query section (B-tree workloads)")
     ap.add_argument("--learned-n", type=int, default=2**30)
     ap.add_argument("--learned-q", type=int, default=2**28)

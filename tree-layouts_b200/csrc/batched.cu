@@ -138,6 +138,10 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
                      BatchTotals tot, Ctrl *ctrl, WaitCfg wc, unsigned int *flags, unsigned int *done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sm = reinterpret_cast<K *>(smem_raw);
+    // the scatter's per-warp queues reuse the tile buffer (a work item is either
+    // a stream tile or a scatter chunk); the launch sizes it for both
+    K *qval = sm;
+    uint16_t *qoff = reinterpret_cast<uint16_t *>(sm + (blockDim.x / 32) * kDeferCap);
     __shared__ unsigned long long s_ticket;
     __shared__ int s_ok;
     __shared__ uint32_t s_j;
@@ -165,7 +169,7 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
             __syncthreads();
             if (!s_ok) continue;
             const BatchInst &I = inst[s_j];
-            btree_scatter_chunk(I.S, keys + I.off, scr + I.scr_base, (c - I.chunk_base) * kScatterChunk);
+            btree_scatter_chunk(I.S, keys + I.off, scr + I.scr_base, (c - I.chunk_base) * kScatterChunk, qval, qoff);
         }
     }
 }
@@ -382,7 +386,8 @@ static int launch_batch_permute(const tl_batch_plan_impl &P, K *keys, char *ws, 
     wc.flag_value = 1;
     wc.wait_value = debug_force_timeout() ? 0xFFFFFFFFu : 1u;
     wc.spin_limit = debug_spin_limit();
-    const size_t smem = (size_t)P.tot.max_tile * sizeof(K) + 16;
+    const size_t queues = (size_t)(threads / 32) * kDeferCap * (sizeof(K) + sizeof(uint16_t));
+    const size_t smem = std::max((size_t)P.tot.max_tile * sizeof(K) + 16, queues);
     auto kern = batch_permute_kernel<K>;
     TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;

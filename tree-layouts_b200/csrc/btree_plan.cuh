@@ -8,10 +8,13 @@
 
 namespace tl {
 
-// Keys per scratch chunk of the scatter pass: kScatterThreads x kScatterUnroll.
+// Scatter pass: chunks of kScatterChunk scratch slots per CTA work item, taken
+// by the block's threads in sub-batches of kScatterUnroll keys per thread.
 constexpr int kScatterThreads = 256;
-constexpr int kScatterUnroll = 16;
-constexpr uint64_t kScatterChunk = (uint64_t)kScatterThreads * kScatterUnroll;
+constexpr int kScatterUnroll = 8;
+constexpr uint64_t kScatterChunk = 16384;
+constexpr int kDeferCap = 32 * kScatterUnroll;  // per-warp queue: one sub-batch never overflows it
+static_assert(kScatterChunk <= 65536, "queued chunk offsets are 16-bit");
 
 // ---------------------------------------------------------------- B-tree stream
 // Two schedules.  Plan R (right to left): the last level's keys go straight to
@@ -193,11 +196,17 @@ struct Regime {
     uint64_t dbase, sbase;
     uint32_t r0, skip;
     int kind;
+    // scatter only: second-level fast path for the keys with rem == skip (one
+    // level up): their index m = q0 + ql + madd, written m = Q1 (b+1) + R1 +
+    // ql, lands at d2base + m - m / (b+1) when m % (b+1) != 0.
+    uint64_t Q1, d2base;
+    uint32_t R1;
+    int two;
 };
 
 TL_HD Regime btree_stream_regime(const BtreeStream &S, uint64_t p0, uint64_t p1) {
     const BtreeGeom &g = S.g;
-    Regime R{0, 0, 0, 0, 0};
+    Regime R{0, 0, 0, 0, 0, 0, 0, 0, 0};
     uint64_t q0, r0;
     if (S.plan == PLAN_L) {
         if (p0 >= g.lir) {
@@ -250,8 +259,20 @@ TL_HD bool btree_regime_place(const BtreeStream &S, const Regime &R, uint32_t o,
 // generic btree_slot_dest).  kind 0: generic for the whole chunk.
 TL_HD Regime btree_scatter_regime(const BtreeStream &S, uint64_t c0, uint64_t c1) {
     const BtreeGeom &g = S.g;
-    Regime R{0, 0, 0, 0, 0};
-    uint64_t q0, r0;
+    Regime R{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t q0, r0, Q1, R1;
+    // The keys with rem == skip sit one level up.  With m their index within
+    // the runs of that level (1-based, m = q0 + ql + madd), the ones with
+    // m % (b+1) != 0 sit at level L2 of the top tree at pw[L2] - 1 + (m - m/(b+1))
+    // - 1 + ... : d2base + m - floor(m/(b+1)).
+    auto second = [&](uint64_t mfirst, uint32_t level_from_root) {
+        if (level_from_root >= 48) return;
+        S.fd.divmod(mfirst, Q1, R1);
+        R.Q1 = Q1;
+        R.R1 = (uint32_t)R1;
+        R.d2base = g.pw[level_from_root] - 2;
+        R.two = 1;
+    };
     if (S.plan == PLAN_R) {
         if (g.h >= 1) {
             S.fd.divmod(c0 + 1, q0, r0);
@@ -259,6 +280,8 @@ TL_HD Regime btree_scatter_regime(const BtreeStream &S, uint64_t c0, uint64_t c1
             R.r0 = (uint32_t)r0;
             R.skip = 0;
             R.dbase = g.pw[g.h - 1] - 2 + q0 * g.b;
+            // rem == 0: c + 1 = M (b+1), M = q0 + ql; level h-2 when M % (b+1) != 0
+            if (g.h >= 2) second(q0, g.h - 2);
         }
     } else if (c1 <= g.l + g.i) {
         S.fd.divmod(c0, q0, r0);
@@ -266,12 +289,17 @@ TL_HD Regime btree_scatter_regime(const BtreeStream &S, uint64_t c0, uint64_t c1
         R.r0 = (uint32_t)r0;
         R.skip = (uint32_t)g.b;
         R.dbase = g.ni + q0 * g.b;
+        // separator of leaf j = q0 + ql: top rank j, c + 1 = j + 1; level h-1
+        // (the top tree's last level) when (j+1) % (b+1) != 0
+        if (g.h >= 1) second(q0 + 1, g.h - 1);
     } else if (c0 >= g.lir && g.h >= 2) {
         S.fd.divmod(c0 - g.lir + S.ibase + 1, q0, r0);
         R.kind = 1;
         R.r0 = (uint32_t)r0;
         R.skip = 0;
         R.dbase = g.pw[g.h - 2] - 2 + q0 * g.b;
+        // mr == 0: M = (mq)(b+1), mq = q0 + ql; level h-3 when mq % (b+1) != 0
+        if (g.h >= 3) second(q0, g.h - 3);
     }
     return R;
 }
@@ -289,6 +317,26 @@ TL_HD uint64_t btree_slot_dest(const BtreeStream &S, uint64_t slot) {
     }
     return btree_pos(g, S.fd, s);
 }
+
+// Destination of scratch slot c0 + o under a kind-1 scatter regime (the
+// generic btree_slot_dest only for keys two or more levels above the fast one).
+TL_HD uint64_t btree_regime_slot_dest(const BtreeStream &S, const Regime &R, uint64_t c0, uint32_t o) {
+    const uint32_t d = S.fd32.d;
+    const uint32_t vv = R.r0 + o;
+    const uint32_t ql = S.fd32.div(vv);
+    if (vv - ql * d != R.skip) return R.dbase + (vv - ql);
+    if (R.two) {
+        const uint32_t w = R.R1 + ql;
+        const uint32_t q2 = S.fd32.div(w);
+        const uint32_t r2 = w - q2 * d;
+        if (r2 != 0) {
+            // m = Q1 (b+1) + w = (Q1 + q2)(b+1) + r2: pos = pw[L] - 1 + (Q1+q2) b + r2 - 1
+            return R.d2base + (R.Q1 + q2) * S.g.b + r2;
+        }
+    }
+    return btree_slot_dest(S, c0 + o);
+}
+
 
 // Tile-local form of btree_slot_dest for the slots of a chunk starting at c0:
 // the division of the chunk's first slot is done once, each slot then divides a
@@ -411,16 +459,28 @@ __device__ __forceinline__ bool btree_stream_tile(const BtreeStream &S, K *__res
     return true;
 }
 
-// Scratch -> final positions for the chunk of kScatterChunk slots at c0: every
-// thread first issues its kScatterUnroll coalesced loads, then its stores, so it
-// keeps that many loads in flight.  Scratch is read through L2 only (.cg).
-template <typename K>
+// Scratch -> final positions for the chunk of kScatterChunk slots at c0.
+// Every thread first issues kScatterUnroll coalesced loads (scratch is read
+// through L2 only), then stores.  Under a kind-1 regime the keys on the fast
+// path are stored directly; the others (one level up and above, at most one in
+// b+1) are queued per warp in shared memory and placed afterwards by the whole
+// warp, so their longer path runs on full warps instead of diverging every
+// step.  Binary trees (b = 1) use the branch-free trailing-zeros position.
+// `qval`/`qoff` hold kDeferCap (value, chunk offset) entries per warp of the
+// block; binary trees never touch them.  kBinaryOnly: the caller guarantees a
+// binary tree under plan R, and only the trailing-zeros path is compiled.
+template <typename K, bool kBinaryOnly = false>
 __device__ __forceinline__ void btree_scatter_chunk(const BtreeStream &S, K *__restrict__ A,
-                                                    const K *__restrict__ scr, uint64_t c0) {
+                                                    const K *__restrict__ scr, uint64_t c0, K *qval,
+                                                    uint16_t *qoff) {
     const uint64_t c1 = min(S.nscratch, c0 + kScatterChunk);
-    const Regime R = btree_scatter_regime(S, c0, c1);
-    const ScatterDiv sd = btree_scatter_div(S, c0);
     const uint32_t cnt = (uint32_t)(c1 - c0);
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    K *wq = qval + warp * kDeferCap;
+    uint16_t *wo = qoff + warp * kDeferCap;
+    const bool binary = kBinaryOnly || (S.g.b == 1 && S.plan == PLAN_R);
+    const Regime R = binary ? Regime{} : btree_scatter_regime(S, c0, c1);
+    const ScatterDiv sd = (binary || R.kind == 1) ? ScatterDiv{} : btree_scatter_div(S, c0);
     const uint32_t d = S.fd32.d;
     for (uint32_t sub = 0; sub < cnt; sub += blockDim.x * kScatterUnroll) {
         K v[kScatterUnroll];
@@ -429,19 +489,42 @@ __device__ __forceinline__ void btree_scatter_chunk(const BtreeStream &S, K *__r
             const uint32_t o = sub + threadIdx.x + u * blockDim.x;
             if (o < cnt) v[u] = __ldcg(scr + c0 + o);
         }
+        if (binary) {
 #pragma unroll
-        for (int u = 0; u < kScatterUnroll; ++u) {
-            const uint32_t o = sub + threadIdx.x + u * blockDim.x;
-            if (o < cnt) {
-                uint64_t dst;
-                if (R.kind == 1) {
+            for (int u = 0; u < kScatterUnroll; ++u) {
+                const uint32_t o = sub + threadIdx.x + u * blockDim.x;
+                if (o < cnt) A[btree_perfect_pos(S.g, S.fd, c0 + o, S.g.h)] = v[u];
+            }
+        } else if (R.kind == 1) {
+            uint32_t nq = 0;  // warp-uniform
+#pragma unroll
+            for (int u = 0; u < kScatterUnroll; ++u) {
+                const uint32_t o = sub + threadIdx.x + u * blockDim.x;
+                bool defer = false;
+                if (o < cnt) {
                     const uint32_t vv = R.r0 + o;
                     const uint32_t ql = S.fd32.div(vv);
-                    dst = vv - ql * d != R.skip ? R.dbase + (vv - ql) : btree_slot_dest(S, c0 + o);
-                } else {
-                    dst = btree_slot_dest_tile(S, sd, c0 + o);
+                    if (vv - ql * d != R.skip)
+                        A[R.dbase + (vv - ql)] = v[u];
+                    else
+                        defer = true;
                 }
-                A[dst] = v[u];
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, defer);
+                if (defer) {
+                    const uint32_t at = nq + __popc(m & ((1u << lane) - 1u));
+                    wq[at] = v[u];
+                    wo[at] = (uint16_t)o;
+                }
+                nq += __popc(m);
+            }
+            __syncwarp();
+            for (uint32_t e = lane; e < nq; e += 32) A[btree_regime_slot_dest(S, R, c0, wo[e])] = wq[e];
+            __syncwarp();
+        } else {
+#pragma unroll
+            for (int u = 0; u < kScatterUnroll; ++u) {
+                const uint32_t o = sub + threadIdx.x + u * blockDim.x;
+                if (o < cnt) A[btree_slot_dest_tile(S, sd, c0 + o)] = v[u];
             }
         }
     }

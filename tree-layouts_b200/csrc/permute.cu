@@ -55,12 +55,17 @@ btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl 
     }
 }
 
-template <typename K>
-__global__ void __launch_bounds__(kScatterThreads)
+// kQueue: the per-warp deferred queues exist (b > 1, or plan L); binary trees
+// under plan R use the branch-free path and no shared memory, which leaves more
+// blocks resident.
+template <typename K, bool kQueue>
+__global__ void __launch_bounds__(kScatterThreads, kQueue ? 6 : 8)
 btree_scatter_kernel(K *__restrict__ A, const K *__restrict__ scr, BtreeStream S) {
+    __shared__ K qval[kQueue ? (kScatterThreads / 32) * kDeferCap : 1];
+    __shared__ uint16_t qoff[kQueue ? (kScatterThreads / 32) * kDeferCap : 1];
     for (uint64_t c0 = (uint64_t)blockIdx.x * kScatterChunk; c0 < S.nscratch;
          c0 += (uint64_t)gridDim.x * kScatterChunk)
-        btree_scatter_chunk(S, A, scr, c0);
+        btree_scatter_chunk<K, !kQueue>(S, A, scr, c0, qval, qoff);
 }
 
 // ---------------------------------------------------------------- mvEB stream
@@ -284,8 +289,11 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
         if (pl.scratch_keys) {
+            int sper = 0;
+            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sper, mveb_scatter_kernel<K>,
+                                                                      kScatterThreads, 0));
             uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterThreads - 1) / kScatterThreads,
-                                             (uint64_t)smx * 8);
+                                             (uint64_t)std::max(sper, 1) * smx);
             mveb_scatter_kernel<K><<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.mp);
             TL_CUDA_TRY(cudaGetLastError());
         }
@@ -299,9 +307,15 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
         if (pl.scratch_keys) {
+            // one wave of resident blocks striding over the chunks: a second,
+            // partial wave would leave the tail of the pass under-occupied
+            const bool queue = !(pl.bs.g.b == 1 && pl.bs.plan == PLAN_R);
+            auto skern = queue ? btree_scatter_kernel<K, true> : btree_scatter_kernel<K, false>;
+            int sper = 0;
+            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sper, skern, kScatterThreads, 0));
             uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterChunk - 1) / kScatterChunk,
-                                             (uint64_t)smx * 8);
-            btree_scatter_kernel<K><<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.bs);
+                                             (uint64_t)std::max(sper, 1) * smx);
+            skern<<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.bs);
             TL_CUDA_TRY(cudaGetLastError());
         }
     }
@@ -470,11 +484,7 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
                 const uint64_t d = btree_slot_dest(pl.bs, c);
                 if (btree_slot_dest_tile(pl.bs, sd, c) != d) ++viol;  // fast path == reference form
                 const Regime RG = btree_scatter_regime(pl.bs, cc0, std::min(pl.bs.nscratch, cc0 + kScatterChunk));
-                if (RG.kind == 1) {
-                    const uint32_t vv = RG.r0 + (uint32_t)(c - cc0);
-                    const uint32_t ql = pl.bs.fd32.div(vv);
-                    if (vv - ql * pl.bs.fd32.d != RG.skip && RG.dbase + (vv - ql) != d) ++viol;
-                }
+                if (RG.kind == 1 && btree_regime_slot_dest(pl.bs, RG, cc0, (uint32_t)(c - cc0)) != d) ++viol;
                 if (d >= n) { ++viol; continue; }
                 A[d] = scr[c];
                 ++pos_writes[d];
