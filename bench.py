@@ -138,19 +138,27 @@ class ClockSampler:
                 "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
+REF_FUNCS = {"bst": "timePermuteBST (cpu/src/bst-involutions.h)",
+             "btree": "timePermuteBtree (cpu/src/btree-cycles.h)"}
+
+
 def cpu_reference_permute(layout, b, n_sample, key_bytes, reps, min_seconds=8.0):
     """The reference's own CPU OpenMP permutation (compiled from its sources into
-    oracle/_ref/libref_cpu.so) on n_sample keys with every host thread; falls back
-    to the oracle's single-thread C restatement when that build is absent."""
+    oracle/_ref/libref_cpu.so) on n_sample uint64 keys with every host thread.
+    The reference has no CPU mvEB (its CPU tree is the standard vEB), and the
+    oracle's single-thread C restatement of its mvEB stands in there, as it does
+    for every layout when that build is absent."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     threads = os.cpu_count() or 1
-    ref = O.ref_cpu()
+    ref = O.ref_cpu() if layout != "mveb" else None
+    kind = "reference" if ref is not None else "port"
+    if ref is None:
+        threads = 1
     A = np.empty(n_sample, dtype=np.uint64)
     times = []
     t_begin = time.time()
-    kind = "reference" if ref is not None else "port"
     for r in range(reps):
         A[:] = np.arange(1, n_sample + 1, dtype=np.uint64)  # initSortedList (untimed)
         if ref is not None:
@@ -158,28 +166,30 @@ def cpu_reference_permute(layout, b, n_sample, key_bytes, reps, min_seconds=8.0)
                 ms = ref.ref_cpu_permute_bst_u64(A, n_sample, threads)
             else:
                 ms = ref.ref_cpu_permute_btree_u64(A, n_sample, b, threads)
+        elif layout == "mveb":
+            t0 = time.perf_counter()
+            O.lib().orc_permute_mveb(A, n_sample)
+            ms = (time.perf_counter() - t0) * 1e3
         else:
-            threads = 1
             ms = O.lib().orc_time_permute_btree(A, n_sample, b if layout != "bst" else 1)
         times.append(ms)
         if time.time() - t_begin > min_seconds and r >= 1:
             break
     ms = statistics.median(times)
-    gbs = 2.0 * n_sample * key_bytes / (ms * 1e-3) / 1e9
+    gbs = 2.0 * n_sample * 8 / (ms * 1e-3) / 1e9
+    what = REF_FUNCS[layout] if ref is not None else f"the oracle's C port of the reference's {layout} permutation"
     return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-            "sample": f"{layout} b={b} n={n_sample} uint64 keys 1..n (initSortedList), median of {len(times)} "
-                      f"runs of timePermuteBtree on {threads} threads ({ms:.1f} ms)"}
+            "sample": f"{layout}{'' if layout != 'btree' else f' b={b}'} n={n_sample} uint64 keys 1..n "
+                      f"(initSortedList), median of {len(times)} runs of {what} on {threads} thread(s) "
+                      f"({ms:.1f} ms); GB/s counts 8-byte keys"}
 
 
 def run_reference(args, rank):
     layout, b, n, kb, *_ = WORKLOADS[args.workload]
     if rank != 0:
         return
-    if layout == "mveb":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU code has no mvEB layout "
-                          "(cpu/src builds the standard vEB); its mvEB exists only as GPU code"}))
-        return
-    n_sample = min(n, args.ref_n) if args.ref_n else n
+    # the single-thread mvEB port runs on a bounded sample (about 2 s a run)
+    n_sample = min(n, args.ref_n) if args.ref_n else (n if layout != "mveb" else min(n, 2**28 - 1))
     steps = []
     for _ in range(args.warmup):
         cpu_reference_permute(layout, b, n_sample, kb, 1, 0)
@@ -190,12 +200,13 @@ def run_reference(args, rank):
     ms = 2.0 * n_sample * 8 / (v * 1e9) * 1e3
     cb = dict(steps[0])
     cb["value"] = v
+    metric = METRIC if layout == "btree" else METRIC.replace("level-order B-tree", layout)
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": args.workload, "n": n, "b": b, "key_bytes": kb, "sample_n": n_sample,
-                   "note": "reference CPU OpenMP timePermuteBtree (cpu/src/btree-cycles.h) on the host cores"},
+                   "note": f"{cb['kind']} CPU permutation on the host cores: {cb['sample']}"},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -365,14 +376,14 @@ def run_ours(args, rank, world, local):
     clocks = ClockSampler(local)
     barrier(world)
     clocks.start()
-    t_stream, t_scatter = [], []
+    t_stream, t_pass2 = [], []
     for _ in range(args.steps):
         a, c = step()
         t_stream.append(a)
-        t_scatter.append(c)
+        t_pass2.append(c)
     barrier(world)
     clk = clocks.stop()
-    step_ms = [a + c for a, c in zip(t_stream, t_scatter)]
+    step_ms = [a + c for a, c in zip(t_stream, t_pass2)]
     ms_local = sum(step_ms) / len(step_ms)
     ms = reduce_max(ms_local, world)
     bytes_step = 2.0 * n * kb
@@ -381,6 +392,12 @@ def run_ours(args, rank, world, local):
     peak, peak_kind = peaks()
     stream_ms = sum(t_stream) / len(t_stream)
     achieved = bytes_step / (stream_ms * 1e-3) / 1e9
+    pass2_ms = sum(t_pass2) / len(t_pass2)
+    skeys = C.c_uint64(0)
+    L.tl_debug_permute_scratch_keys.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64)]
+    if L.tl_debug_permute_scratch_keys(lay, n, b or 16, kb, C.byref(skeys)):
+        raise RuntimeError("tl_debug_permute_scratch_keys")
+    pass2_bytes = 2.0 * skeys.value * kb
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"stream_traffic_{args.workload}.json")
     if os.path.exists(prof):
@@ -442,7 +459,7 @@ def run_ours(args, rank, world, local):
         bat = batched_section(args, dev)
 
     cpu = None
-    if rank == 0 and world == 1 and args.cpu_sample > 0 and layout != "mveb":
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
         cpu = cpu_reference_permute(layout, b, min(n, args.cpu_sample), kb, 5)
 
     if rank == 0:
@@ -456,11 +473,14 @@ def run_ours(args, rank, world, local):
                        "l2": "inputs larger than L2 (no flush needed)",
                        "restore": "array re-initialised from a pristine copy between steps, untimed",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
-            "roofline": {"bound": "hbm", "kernel": f"{layout}_stream_kernel", "achieved": round(achieved, 1),
-                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "peak_source": f"hbm_gbs of {peak_kind}", "traffic": traffic,
-                         "algorithmic_bytes_per_launch": int(bytes_step),
-                         "stream_ms": round(stream_ms, 4), "scatter_ms": round(sum(t_scatter) / len(t_scatter), 4),
+            "roofline": {"bound": "hbm", "kernel": "mveb_stream_kernel" if layout == "mveb" else "btree_stream_kernel",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": f"hbm_gbs of {peak_kind}",
+                         "traffic": traffic, "algorithmic_bytes_per_launch": int(bytes_step),
+                         "stream_ms": round(stream_ms, 4),
+                         "pass2_kernel": "mveb_scatter_kernel" if layout == "mveb" else "btree_copy_kernel",
+                         "pass2_ms": round(pass2_ms, 4), "pass2_bytes_per_launch": int(pass2_bytes),
+                         "pass2_achieved": round(pass2_bytes / (pass2_ms * 1e-3) / 1e9, 1) if pass2_ms > 0 else None,
                          "whole_permute_frac": round(bytes_step / (ms_local * 1e-3) / 1e9 / peak, 4)},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -183,7 +183,8 @@ int tl_batch_query(const tl_batch_plan *plan, const void *dev_keys, const void *
                    const uint32_t *dev_inst, uint64_t q, uint64_t *dev_answers, void *dev_workspace,
                    uint64_t workspace_bytes, void *stream, float *ms);
 /* Tuning per size class c = floor(log2 n_j), 48 entries each: keys per stream
- * tile, top levels pinned in shared memory by the query; plus the query work
+ * tile (a power of two, 256 .. 96 KB / key_bytes), top levels pinned in shared
+ * memory by the query; plus the query work
  * item and the permute block size (256 or 512); 0 / NULL keeps a value.
  * Changing tile sizes rebuilds the plan from dev_offsets. */
 int tl_batch_set_tuning(tl_batch_plan *plan, const uint32_t *tile_keys, const uint32_t *pin_levels,
@@ -277,8 +278,12 @@ int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_
 int tl_debug_struct_size(int which);
 /* Schedule the B-tree permutation uses for (n, b): 0 right-to-left, 1 left-to-right. */
 int tl_debug_btree_plan(uint64_t n, uint64_t b);
+/* Keys the permutation of (layout, n, b, key_bytes) moves through its scratch
+ * buffer (the second pass reads and writes each once). */
+int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
 /* tl_permute with library-allocated workspace, reporting the device time of its
- * two passes: phase_ms[0] = setup + stream kernel, phase_ms[1] = scatter kernel. */
+ * two passes: phase_ms[0] = setup + stream kernel, phase_ms[1] = the second pass
+ * (B-tree: scratch copy kernel; mvEB: scratch scatter kernel). */
 int tl_debug_permute_phases(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                             void *stream, float *phase_ms);
 

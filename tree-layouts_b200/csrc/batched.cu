@@ -5,14 +5,15 @@
 //
 // Plan (built once per offset table, on the device): a setup kernel computes
 // every instance's geometry and schedule (the same host/device helpers as the
-// single-array path), its tile count, scratch size and scatter-chunk count, and
-// exclusive prefix sums of them.  Execute: a memset of the control words and one
+// single-array path), its tile count, scratch size and copy-chunk count, and
+// exclusive prefix sums of them; a second kernel writes the owner instance of
+// every tile and copy chunk.  Execute: a memset of the control words and one
 // persistent kernel; tickets 0..T-1 are stream tiles (instance by instance, each
-// in its own plan's direction), tickets T.. are scatter chunks.  A chunk of
-// instance j starts once all of j's tiles have stored (a per-instance counter,
-// bounded wait); stream tiles never wait on chunks, so every wait ends.
-// Per size class (floor(log2 n_j)) the tile size comes from a tuning table that
-// tl_batch_autotune fills by measurement.
+// in its own plan's direction), tickets T.. are copy chunks (scratch -> final
+// positions).  A chunk of instance j starts once all of j's tiles have stored
+// (a per-instance counter, bounded wait); stream tiles never wait on chunks, so
+// every wait ends.  Per size class (floor(log2 n_j)) the tile size comes from a
+// tuning table that tl_batch_autotune fills by measurement.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -28,14 +29,15 @@ constexpr int kBatchThreads = 256;     // query kernel
 constexpr int kBatchMaxThreads = 512;  // permute kernel: 256 or 512 (tuned)
 constexpr int kMaxClass = 48;
 
-struct BatchInst {
+struct alignas(16) BatchInst {
     BtreeStream S;
     uint64_t off;          // first key of the instance
     uint64_t tile_base;    // first global tile
-    uint64_t scr_base;     // first scratch slot
-    uint64_t chunk_base;   // first global scatter chunk
+    uint64_t scr_base;     // first scratch slot (same 16-byte offset as the instance's keys)
+    uint64_t chunk_base;   // first global copy chunk
     uint64_t nchunks;
 };
+static_assert(sizeof(BatchInst) % 16 == 0, "BatchInst is copied to shared memory in 16-byte words");
 
 struct BatchTotals {
     uint64_t tiles, chunks, scratch, max_tile;
@@ -50,19 +52,23 @@ struct tl_batch_plan_impl {
     uint32_t pin_levels[kMaxClass];  // query: top levels pinned in shared memory per size class
     uint32_t query_chunk = 2048;     // queries per CTA work item
     uint32_t threads = 256;          // permute kernel block size
+    uint32_t *owner = nullptr;   // device: owner instance of every tile, then of every copy chunk
     uint64_t off_flags = 0, off_done = 0, off_ctrl = 0, ws_bytes = 0;
     uint64_t total_keys = 0;
 };
 
 // ---------------------------------------------------------------- setup
-__global__ void __launch_bounds__(256) batch_setup_kernel(const int64_t *__restrict__ offsets, uint32_t num, uint64_t b, FastDiv64 fd,
-                                   FastDiv32 fd32, const uint32_t *__restrict__ tile_keys,
-                                   BatchInst *__restrict__ inst, BatchTotals *__restrict__ tot) {
+__global__ void __launch_bounds__(256) batch_setup_kernel(const int64_t *__restrict__ offsets, uint32_t num, uint64_t b,
+                                                          uint32_t key_bytes, FastDiv64 fd, FastDiv32 fd32,
+                                                          FastDiv32 fd32b, const __grid_constant__ PowDivs pdivs,
+                                                          const uint32_t *__restrict__ tile_keys,
+                                                          BatchInst *__restrict__ inst, BatchTotals *__restrict__ tot) {
     // one block: per-instance plans, then exclusive scans in instance order
     __shared__ unsigned long long s_part[3][1024];
     const uint32_t T = blockDim.x;
     const uint32_t per = (num + T - 1) / T;
     const uint32_t j0 = threadIdx.x * per, j1 = min(num, j0 + per);
+    const uint64_t vec = 16 / key_bytes;
     unsigned long long st = 0, ss = 0, sc = 0;
     for (uint32_t j = j0; j < j1; ++j) {
         BatchInst I;
@@ -72,17 +78,25 @@ __global__ void __launch_bounds__(256) batch_setup_kernel(const int64_t *__restr
         I.S.g = make_btree_geom(n, b);
         I.S.fd = fd;
         I.S.fd32 = fd32;
+        I.S.fd32b = fd32b;
+        btree_set_pow_divs(I.S, pdivs);
         const uint32_t cls = n ? bit_length(n) - 1 : 0;
-        I.S.tile_keys = tile_keys[cls < kMaxClass ? cls : kMaxClass - 1];
+        I.S.tile_keys = tile_keys[cls < kMaxClass ? cls : kMaxClass - 1];  // a power of two
+        I.S.tile_shift = (uint32_t)__ffsll((long long)I.S.tile_keys) - 1;
         I.S.ntiles = (n + I.S.tile_keys - 1) / I.S.tile_keys;
-        btree_choose_plan(I.S);
+        btree_choose_plan(I.S, key_bytes);
         if (n <= 1) {
             I.S.ntiles = 0;
             I.S.nscratch = 0;
         }
-        I.nchunks = (I.S.nscratch + kScatterChunk - 1) / kScatterChunk;
+        uint64_t ncopy = 0;
+        for (int k = 0; k < btree_copy_range_count(I.S); ++k) {
+            CopyRange r;
+            if (btree_copy_range(I.S, k, r)) ncopy += r.len;
+        }
+        I.nchunks = I.S.nscratch ? (ncopy + kCopyChunk - 1) / kCopyChunk : 0;
         st += I.S.ntiles;
-        ss += I.S.nscratch;
+        ss += I.S.nscratch ? I.S.nscratch + vec - 1 : 0;  // room to align the base
         sc += I.nchunks;
         inst[j] = I;
     }
@@ -111,65 +125,84 @@ __global__ void __launch_bounds__(256) batch_setup_kernel(const int64_t *__restr
     __syncthreads();
     unsigned long long bt = s_part[0][threadIdx.x], bs = s_part[1][threadIdx.x], bc = s_part[2][threadIdx.x];
     for (uint32_t j = j0; j < j1; ++j) {
+        const uint64_t ns = inst[j].S.nscratch;
         inst[j].tile_base = bt;
-        inst[j].scr_base = bs;
+        inst[j].scr_base = bs + ((inst[j].off % vec) + vec - (bs % vec)) % vec;
         inst[j].chunk_base = bc;
         bt += inst[j].S.ntiles;
-        bs += inst[j].S.nscratch;
+        bs += ns ? ns + vec - 1 : 0;
         bc += inst[j].nchunks;
     }
 }
 
-// Last instance j with field(j) <= x (fields ascend with j).
-template <typename F>
-__device__ __forceinline__ uint32_t find_inst(const BatchInst *inst, uint32_t num, uint64_t x, F field) {
-    uint32_t lo = 0, hi = num - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        if (field(inst[mid]) <= x) lo = mid; else hi = mid - 1;
+// owner[t] = instance of tile t (t < tiles); owner[tiles + c] = instance of copy chunk c.
+__global__ void batch_owner_kernel(const BatchInst *__restrict__ inst, uint32_t num, uint64_t tiles,
+                                   uint32_t *__restrict__ owner) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t j = w0; j < num; j += nw) {
+        const BatchInst &I = inst[j];
+        for (uint64_t t = lane; t < I.S.ntiles; t += 32) owner[I.tile_base + t] = (uint32_t)j;
+        for (uint64_t c = lane; c < I.nchunks; c += 32) owner[tiles + I.chunk_base + c] = (uint32_t)j;
     }
-    return lo;
 }
 
 // ---------------------------------------------------------------- permute
 template <typename K>
-__global__ void __launch_bounds__(kBatchMaxThreads, 1)
-batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst *__restrict__ inst, uint32_t num,
-                     BatchTotals tot, Ctrl *ctrl, WaitCfg wc, unsigned int *flags, unsigned int *done) {
+__global__ void __launch_bounds__(kBatchMaxThreads, 2)
+batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst *__restrict__ inst,
+                     const uint32_t *__restrict__ owner, BatchTotals tot, Ctrl *ctrl, WaitCfg wc,
+                     unsigned int *flags, unsigned int *done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sm = reinterpret_cast<K *>(smem_raw);
-    // the scatter's per-warp queues reuse the tile buffer (a work item is either
-    // a stream tile or a scatter chunk); the launch sizes it for both
-    K *qval = sm;
-    uint16_t *qoff = reinterpret_cast<uint16_t *>(sm + (blockDim.x / 32) * kDeferCap);
     __shared__ unsigned long long s_ticket;
     __shared__ int s_ok;
     __shared__ uint32_t s_j;
-    for (;;) {
-        const unsigned long long t = next_ticket(ctrl, &s_ticket);
-        if (t >= tot.tiles + tot.chunks) break;
-        if (t < tot.tiles) {
-            if (threadIdx.x == 0) s_j = find_inst(inst, num, t, [](const BatchInst &I) { return I.tile_base; });
-            __syncthreads();
-            const BatchInst &I = inst[s_j];
+    __shared__ __align__(16) unsigned char s_inst_raw[sizeof(BatchInst)];
+    __shared__ TileShared ts;
+    const BatchInst &I = *reinterpret_cast<const BatchInst *>(s_inst_raw);
+    TicketPipe tp;
+    for (unsigned long long t = ticket_first(ctrl, &s_ticket); t < tot.tiles + tot.chunks;
+         t = ticket_advance(tp, &s_ticket)) {
+        ticket_claim(ctrl, tp);
+        const bool is_tile = t < tot.tiles;
+        if (threadIdx.x == 0) {
+            s_j = owner[t];
+            s_ok = 1;
+            if (!is_tile) s_ok = wait_flag(&done[s_j], (unsigned int)inst[s_j].S.ntiles, ctrl, wc) ? 1 : 0;
+        }
+        __syncthreads();
+        {  // the owner's plan into shared memory: every thread reads it many times
+            const uint4 *src = reinterpret_cast<const uint4 *>(inst + s_j);
+            uint4 *dst = reinterpret_cast<uint4 *>(s_inst_raw);
+            for (uint32_t w = threadIdx.x; w < sizeof(BatchInst) / 16; w += blockDim.x) dst[w] = src[w];
+        }
+        __syncthreads();
+        if (!s_ok) continue;
+        if (is_tile) {
             const uint64_t k = btree_tile_of_ticket(I.S, t - I.tile_base);
-            btree_stream_tile(I.S, keys + I.off, scr + I.scr_base, flags + I.tile_base, ctrl, wc, k, sm, &s_ok);
+            btree_stream_tile(I.S, keys + I.off, scr + I.scr_base, flags + I.tile_base, ctrl, wc, k, sm, ts);
             __syncthreads();  // every store of the tile issued before it counts as done
             if (threadIdx.x == 0) {
                 __threadfence();
                 atomicAdd(&done[s_j], 1u);
             }
         } else {
-            const uint64_t c = t - tot.tiles;
-            if (threadIdx.x == 0) {
-                s_j = find_inst(inst, num, c, [](const BatchInst &I) { return I.chunk_base; });
-                const unsigned int need = (unsigned int)inst[s_j].S.ntiles;
-                s_ok = wait_flag(&done[s_j], need, ctrl, wc) ? 1 : 0;
+            // one chunk of the instance's copy ranges, taken as one concatenated range
+            const uint64_t lo = (t - tot.tiles - I.chunk_base) * kCopyChunk, hi = lo + kCopyChunk;
+            uint64_t acc = 0;
+            const int nr = btree_copy_range_count(I.S);
+            for (int q = 0; q < nr && acc < hi; ++q) {
+                CopyRange r;
+                if (!btree_copy_range(I.S, q, r)) continue;
+                const uint64_t a = lo > acc ? lo - acc : 0;
+                const uint64_t e = min(hi - acc, r.len);
+                if (a < e)
+                    copy_keys(keys + I.off + r.dst + a, scr + I.scr_base + r.src + a, e - a, threadIdx.x,
+                              blockDim.x);
+                acc += r.len;
             }
-            __syncthreads();
-            if (!s_ok) continue;
-            const BatchInst &I = inst[s_j];
-            btree_scatter_chunk(I.S, keys + I.off, scr + I.scr_base, (c - I.chunk_base) * kScatterChunk, qval, qoff);
         }
     }
 }
@@ -317,8 +350,10 @@ static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStr
     TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_tk), sizeof(P.tile_keys), st));
     TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_tot), sizeof(BatchTotals), st));
     TL_CUDA_TRY(cudaMemcpyAsync(d_tk, P.tile_keys, sizeof(P.tile_keys), cudaMemcpyHostToDevice, st));
-    batch_setup_kernel<<<1, 256, 0, st>>>(dev_offsets, P.num, P.b, FastDiv64(P.b + 1), FastDiv32((uint32_t)(P.b + 1)),
-                                           d_tk, P.inst, d_tot);
+    batch_setup_kernel<<<1, 256, 0, st>>>(dev_offsets, P.num, P.b, P.key_bytes, FastDiv64(P.b + 1),
+                                           FastDiv32((uint32_t)(P.b + 1)),
+                                           P.b >= 2 ? FastDiv32((uint32_t)P.b) : FastDiv32(), make_pow_divs(P.b), d_tk,
+                                           P.inst, d_tot);
     TL_CUDA_TRY(cudaGetLastError());
     int64_t last = 0;
     TL_CUDA_TRY(cudaMemcpyAsync(&P.tot, d_tot, sizeof(BatchTotals), cudaMemcpyDeviceToHost, st));
@@ -327,8 +362,19 @@ static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStr
     cudaFreeAsync(d_tk, st);
     cudaFreeAsync(d_tot, st);
     P.total_keys = (uint64_t)last;
+    if (P.owner) cudaFreeAsync(P.owner, st);
+    P.owner = nullptr;
+    const uint64_t nowner = P.tot.tiles + P.tot.chunks;
+    if (nowner) {
+        TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&P.owner), nowner * sizeof(uint32_t), st));
+        const unsigned g = (unsigned)std::min<uint64_t>(((uint64_t)P.num * 32 + 255) / 256, (uint64_t)batch_sms() * 8);
+        batch_owner_kernel<<<g, 256, 0, st>>>(P.inst, P.num, P.tot.tiles, P.owner);
+        TL_CUDA_TRY(cudaGetLastError());
+        TL_CUDA_TRY(cudaStreamSynchronize(st));  // the plan is complete when this returns, for any stream
+    }
     auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
-    P.off_flags = al(P.tot.scratch * P.key_bytes);
+    // + 16 bytes: the scratch starts at the keys' own offset within 16 bytes
+    P.off_flags = al(P.tot.scratch * P.key_bytes + 16);
     P.off_done = P.off_flags + al(P.tot.tiles * sizeof(unsigned int));
     P.off_ctrl = P.off_done + al((uint64_t)P.num * sizeof(unsigned int));
     P.ws_bytes = P.off_ctrl + al(sizeof(Ctrl));
@@ -352,6 +398,7 @@ int batch_plan_create(const int64_t *dev_offsets, uint32_t num, uint64_t b, uint
     int rc = build_plan(*P, dev_offsets, st);
     if (rc) {
         cudaFree(P->inst);
+        if (P->owner) cudaFree(P->owner);
         delete P;
         return rc;
     }
@@ -363,6 +410,7 @@ int batch_plan_destroy(tl_batch_plan *plan) {
     if (!plan) return TL_ERROR_INVALID_VALUE;
     auto *P = reinterpret_cast<tl_batch_plan_impl *>(plan);
     cudaFree(P->inst);
+    if (P->owner) cudaFree(P->owner);
     delete P;
     return TL_SUCCESS;
 }
@@ -375,7 +423,8 @@ int batch_workspace_bytes(const tl_batch_plan *plan, uint64_t *bytes) {
 
 template <typename K>
 static int launch_batch_permute(const tl_batch_plan_impl &P, K *keys, char *ws, cudaStream_t st, int threads) {
-    K *scr = reinterpret_cast<K *>(ws);
+    // every instance's scratch base shares its keys' offset within 16 bytes
+    K *scr = reinterpret_cast<K *>(ws + (reinterpret_cast<uintptr_t>(keys) & 15));
     unsigned int *flags = reinterpret_cast<unsigned int *>(ws + P.off_flags);
     unsigned int *done = reinterpret_cast<unsigned int *>(ws + P.off_done);
     Ctrl *ctrl = reinterpret_cast<Ctrl *>(ws + P.off_ctrl);
@@ -386,8 +435,7 @@ static int launch_batch_permute(const tl_batch_plan_impl &P, K *keys, char *ws, 
     wc.flag_value = 1;
     wc.wait_value = debug_force_timeout() ? 0xFFFFFFFFu : 1u;
     wc.spin_limit = debug_spin_limit();
-    const size_t queues = (size_t)(threads / 32) * kDeferCap * (sizeof(K) + sizeof(uint16_t));
-    const size_t smem = std::max((size_t)P.tot.max_tile * sizeof(K) + 16, queues);
+    const size_t smem = (size_t)P.tot.max_tile * sizeof(K) + 16;  // the largest tile plus its 16-byte head slack
     auto kern = batch_permute_kernel<K>;
     TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -395,7 +443,7 @@ static int launch_batch_permute(const tl_batch_plan_impl &P, K *keys, char *ws, 
     const uint64_t work = P.tot.tiles + P.tot.chunks;
     if (work == 0) return TL_SUCCESS;
     const uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * batch_sms(), work);
-    kern<<<(unsigned)grid, threads, smem, st>>>(keys, scr, P.inst, P.num, P.tot, ctrl, wc, flags, done);
+    kern<<<(unsigned)grid, threads, smem, st>>>(keys, scr, P.inst, P.owner, P.tot, ctrl, wc, flags, done);
     TL_CUDA_TRY(cudaGetLastError());
     return TL_SUCCESS;
 }
@@ -502,7 +550,7 @@ int batch_set_tuning(tl_batch_plan *plan, const uint32_t *tile_keys, const uint3
     if (tile_keys) {
         for (int c = 0; c < kMaxClass; ++c) {
             const uint32_t t = tile_keys[c];
-            if (t < 256 || t * P.key_bytes > 96 * 1024 || t % 16) return TL_ERROR_INVALID_VALUE;
+            if (t < 256 || t * P.key_bytes > 96 * 1024 || (t & (t - 1))) return TL_ERROR_INVALID_VALUE;
         }
         memcpy(P.tile_keys, tile_keys, sizeof(P.tile_keys));
         if (!dev_offsets) return TL_ERROR_INVALID_VALUE;

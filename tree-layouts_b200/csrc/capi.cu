@@ -120,6 +120,10 @@ int tl_debug_struct_size(int which) {
 // stream, top tree via scratch; 1: left-to-right stream, last level via scratch).
 int tl_debug_btree_plan(uint64_t n, uint64_t b) { return btree_plan_of(n, b); }
 
+int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys) {
+    return permute_scratch_keys(layout, n, b, key_bytes, keys);
+}
+
 // Test hook: host replay of the permutation's tile schedule (see emulate_permute).
 int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations) {
     if (n > 0 && !host_A) return TL_ERROR_INVALID_VALUE;

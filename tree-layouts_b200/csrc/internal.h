@@ -82,6 +82,7 @@ int sync_and_check(cudaStream_t st);
 
 int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
 int btree_plan_of(uint64_t n, uint64_t b);
+int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
 int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations);
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
             uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms = nullptr);

@@ -7,15 +7,16 @@
 // therefore done in two kernels instead of the reference's chain of cycle-leader
 // and reversal launches:
 //
-//  1. stream: one pass over the array from the right end to the left, one tile
-//     per ticket.  A tile is read into shared memory, flagged as read, and its
-//     bulk keys are stored straight to their final positions once the tiles
-//     under those positions have been read.  Separators go to a scratch buffer.
-//  2. scatter: the scratch buffer is written to its final positions (out of
-//     place, every destination is free by then).
+//  1. stream: one pass over the array, one tile per ticket.  A tile is read
+//     into shared memory, flagged as read, and its bulk keys are stored
+//     straight to their final positions once the tiles under those positions
+//     have been read.  The other keys go to a scratch buffer.
+//  2. B-tree: a copy of the scratch (indexed by final position) into place;
+//     mvEB: a scatter of the scratch slots to their final positions.  Every
+//     destination is free by then.
 //
-// DRAM traffic is 2*n*w for the stream plus 2*w per separator: n/(b+1)
-// separators for a perfect B-tree, about n/2^8 for an mvEB.
+// DRAM traffic is 2*n*w for the stream plus 2*w per scratch key: n/(b+1) for a
+// perfect B-tree, about n/2^8 for an mvEB.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -31,6 +32,7 @@
 namespace tl {
 
 constexpr int kStreamThreads = 256;
+constexpr int kStreamBlocksPerSM = 6;  // what shared memory allows with 32 KB tiles
 constexpr uint32_t kUnitMaxLevels = 8;
 
 template <typename K>
@@ -41,31 +43,31 @@ constexpr uint64_t stream_tile_keys() {
 static inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 template <typename K>
-__global__ void __launch_bounds__(kStreamThreads)
-btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, BtreeStream S, Ctrl *ctrl, WaitCfg wc,
-                    unsigned int *flags) {
+__global__ void __launch_bounds__(kStreamThreads, kStreamBlocksPerSM)
+btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant__ BtreeStream S, Ctrl *ctrl,
+                    WaitCfg wc, unsigned int *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sm = reinterpret_cast<K *>(smem_raw);
     __shared__ unsigned long long s_ticket;
-    __shared__ int s_ok;
-    for (;;) {
-        unsigned long long t = next_ticket(ctrl, &s_ticket);
-        if (t >= S.ntiles) break;
-        btree_stream_tile(S, A, scr, flags, ctrl, wc, btree_tile_of_ticket(S, t), sm, &s_ok);
+    __shared__ TileShared ts;
+    TicketPipe tp;
+    for (unsigned long long t = ticket_first(ctrl, &s_ticket); t < S.ntiles; t = ticket_advance(tp, &s_ticket)) {
+        ticket_claim(ctrl, tp);
+        btree_stream_tile(S, A, scr, flags, ctrl, wc, btree_tile_of_ticket(S, t), sm, ts);
     }
 }
 
-// kQueue: the per-warp deferred queues exist (b > 1, or plan L); binary trees
-// under plan R use the branch-free path and no shared memory, which leaves more
-// blocks resident.
-template <typename K, bool kQueue>
-__global__ void __launch_bounds__(kScatterThreads, kQueue ? 6 : 8)
-btree_scatter_kernel(K *__restrict__ A, const K *__restrict__ scr, BtreeStream S) {
-    __shared__ K qval[kQueue ? (kScatterThreads / 32) * kDeferCap : 1];
-    __shared__ uint16_t qoff[kQueue ? (kScatterThreads / 32) * kDeferCap : 1];
-    for (uint64_t c0 = (uint64_t)blockIdx.x * kScatterChunk; c0 < S.nscratch;
-         c0 += (uint64_t)gridDim.x * kScatterChunk)
-        btree_scatter_chunk<K, !kQueue>(S, A, scr, c0, qval, qoff);
+// Second pass of a B-tree permutation: the scratch ranges to their final
+// positions, a plain copy (scratch is indexed by final position).
+template <typename K>
+__global__ void __launch_bounds__(kScatterThreads)
+btree_copy_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_constant__ BtreeStream S) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    const int nr = btree_copy_range_count(S);
+    for (int j = 0; j < nr; ++j) {
+        CopyRange r;
+        if (btree_copy_range(S, j, r)) copy_keys(A + r.dst, scr + r.src, r.len, tid, nth);
+    }
 }
 
 // ---------------------------------------------------------------- mvEB stream
@@ -128,7 +130,7 @@ TL_HD uint64_t mveb_slot_rank(const MvebPlan &P, uint64_t s) {
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kStreamThreads)
+__global__ void __launch_bounds__(kStreamThreads, kStreamBlocksPerSM)
 mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant__ MvebParams prm,
                    Ctrl *ctrl, WaitCfg wc, unsigned int *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -139,9 +141,10 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
     const MvebPlan &P = prm.plan;
     const uint64_t ntiles = P.total_tiles;
     int loaded_U = -1;
-    for (;;) {
-        unsigned long long t = next_ticket(ctrl, &s_ticket);
-        if (t >= ntiles) break;
+    const uint32_t lane = threadIdx.x & 31;
+    TicketPipe tp;
+    for (unsigned long long t = ticket_first(ctrl, &s_ticket); t < ntiles; t = ticket_advance(tp, &s_ticket)) {
+        ticket_claim(ctrl, tp);
         const uint64_t k = ntiles - 1 - t;
         int ri;
         uint64_t p0, p1;
@@ -167,12 +170,13 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
         const uint64_t u = (1ull << U) - 1;
         uint64_t g0, g1;
         mveb_tile_groups(R, p0, p1, g0, g1);
-        const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+        const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
         for (uint64_t gi = g0 + warp; gi < g1; gi += nwarps) {
-            const uint64_t gsrc = R.src + (gi << U) - base;
+            const uint32_t gsrc = (uint32_t)(R.src + (gi << U) - base);
             const uint64_t dst = mveb_unit_dst(R, gi);
             for (uint32_t q = lane; q < u; q += 32) A[dst + q] = sm[gsrc + s_inv[q]];
-            if (lane == 0 && R.src + (gi << U) + u < R.src + R.len) scr[R.slot_base + gi] = sm[gsrc + u];
+            if (lane == 0 && R.src + (gi << U) + u < R.src + R.len)
+                scr[R.slot_base + gi] = sm[gsrc + u];
         }
     }
 }
@@ -240,15 +244,21 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
     } else {
         if (b >= (1ull << 31)) return TL_ERROR_UNSUPPORTED;
         pl.bs.g = make_btree_geom(n, b);
+        // per-level tables and 32-bit tile indices of the wait lists
+        if (pl.bs.g.h > (uint32_t)kMaxTopLevels || n / pl.tile_keys >= (1ull << 32)) return TL_ERROR_UNSUPPORTED;
         pl.bs.fd = FastDiv64(b + 1);
         pl.bs.fd32 = FastDiv32((uint32_t)(b + 1));
+        if (b >= 2) pl.bs.fd32b = FastDiv32((uint32_t)b);
         pl.bs.tile_keys = pl.tile_keys;
+        pl.bs.tile_shift = (uint32_t)__builtin_ctzll(pl.tile_keys);
+        btree_set_pow_divs(pl.bs, make_pow_divs(b));
         pl.ntiles = (n + pl.tile_keys - 1) / pl.tile_keys;
         pl.bs.ntiles = pl.ntiles;
-        btree_choose_plan(pl.bs);
+        btree_choose_plan(pl.bs, key_bytes);
         pl.scratch_keys = pl.bs.nscratch;
     }
-    pl.off_flags = align_up(pl.scratch_keys * key_bytes, 256);
+    // + 16 bytes: the scratch starts at the array's own offset within 16 bytes
+    pl.off_flags = align_up(pl.scratch_keys * key_bytes + 16, 256);
     pl.off_ctrl = pl.off_flags + align_up(pl.ntiles * sizeof(unsigned int), 256);
     pl.bytes = pl.off_ctrl + align_up(sizeof(Ctrl), 256);
     return TL_SUCCESS;
@@ -268,7 +278,8 @@ static int sm_count() {
 
 template <typename K>
 static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st, EventTimer &timer) {
-    K *scr = reinterpret_cast<K *>(ws);
+    // the scratch shares A's offset within 16 bytes, so the copy pass vectorises
+    K *scr = reinterpret_cast<K *>(ws + (reinterpret_cast<uintptr_t>(A) & 15));
     unsigned int *flags = reinterpret_cast<unsigned int *>(ws + pl.off_flags);
     Ctrl *ctrl = reinterpret_cast<Ctrl *>(ws + pl.off_ctrl);
     WaitCfg wc;
@@ -277,7 +288,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
     wc.spin_limit = debug_spin_limit();
     // flags and control block are contiguous: one stream-ordered memset clears both
     TL_CUDA_TRY(cudaMemsetAsync(flags, 0, pl.bytes - pl.off_flags, st));
-    const size_t smem = (size_t)pl.tile_keys * sizeof(K) + 16;
+    const size_t smem = (size_t)pl.tile_keys * sizeof(K) + 16;  // the tile plus its 16-byte head slack
     const int smx = sm_count();
     if (pl.layout == TL_LAYOUT_MVEB) {
         auto kern = mveb_stream_kernel<K>;
@@ -307,15 +318,14 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
         if (pl.scratch_keys) {
-            // one wave of resident blocks striding over the chunks: a second,
-            // partial wave would leave the tail of the pass under-occupied
-            const bool queue = !(pl.bs.g.b == 1 && pl.bs.plan == PLAN_R);
-            auto skern = queue ? btree_scatter_kernel<K, true> : btree_scatter_kernel<K, false>;
-            int sper = 0;
-            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sper, skern, kScatterThreads, 0));
-            uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterChunk - 1) / kScatterChunk,
-                                             (uint64_t)std::max(sper, 1) * smx);
-            skern<<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.bs);
+            // resident blocks striding over the copy, 4 vectors in flight per thread
+            int cper = 0;
+            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cper, btree_copy_kernel<K>,
+                                                                      kScatterThreads, 0));
+            const uint64_t per_block = (uint64_t)kScatterThreads * 4 * (16 / sizeof(K));
+            uint64_t cg = std::min<uint64_t>((pl.scratch_keys + per_block - 1) / per_block,
+                                             (uint64_t)std::max(cper, 1) * smx);
+            btree_copy_kernel<K><<<(unsigned)std::max<uint64_t>(cg, 1), kScatterThreads, 0, st>>>(A, scr, pl.bs);
             TL_CUDA_TRY(cudaGetLastError());
         }
     }
@@ -342,6 +352,22 @@ int btree_plan_of(uint64_t n, uint64_t b) {
     PermutePlan pl;
     if (make_plan(TL_LAYOUT_BTREE, n, b, 8, pl)) return -1;
     return pl.bs.plan;
+}
+
+int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys) {
+    if (!keys) return TL_ERROR_INVALID_VALUE;
+    PermutePlan pl;
+    int rc = make_plan(layout, n, b, key_bytes, pl);
+    if (rc) return rc;
+    if (layout == TL_LAYOUT_MVEB) {
+        *keys = pl.mp.plan.total_slots;
+    } else {
+        *keys = 0;
+        CopyRange r;
+        for (int j = 0; j < btree_copy_range_count(pl.bs); ++j)
+            if (btree_copy_range(pl.bs, j, r)) *keys += r.len;
+    }
+    return TL_SUCCESS;
 }
 
 int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes) {
@@ -400,9 +426,10 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
 // already overwritten, a store outside the tile's own source that is not covered
 // by the tiles it waits for, a wait on a tile with a later ticket, and a final
 // position or scratch slot written other than exactly once.  Test hook only.
-int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations) {
+static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *A,
+                              uint64_t *violations) {
     PermutePlan pl;
-    int rc = make_plan(layout, n, b, 8, pl);
+    int rc = make_plan(layout, n, b, key_bytes, pl);
     if (rc) return rc;
     uint64_t viol = 0;
     if (n > 1) {
@@ -444,16 +471,80 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
                 ++slot_writes[s];
             };
             if (!mv) {
-                const TileDiv td = btree_tile_div(pl.bs, p0);
-                const Regime RG = btree_stream_regime(pl.bs, p0, p1);
-                for (uint64_t x = p0; x < p1; ++x) {
-                    uint64_t idx, idx2, idx3;
-                    const bool direct = btree_place_tile(pl.bs, td, x, idx);
-                    if (direct != btree_place(pl.bs, x, idx2) || idx != idx2) ++viol;  // fast path == reference form
-                    if (RG.kind && (btree_regime_place(pl.bs, RG, (uint32_t)(x - p0), idx3) != direct || idx3 != idx))
-                        ++viol;
-                    if (direct) W(idx, tile[x - p0]); else SC(idx, tile[x - p0]);
+                const BtreeStream &S = pl.bs;
+                const Regime RG = btree_stream_regime(S, p0, p1);
+                const uint32_t cnt = (uint32_t)(p1 - p0);
+                // the runs in slot order, as warp 0 computes them, and the wait list
+                TopGroup G0{}, G1{};
+                const int ng = btree_stream_groups(S, p0, p1, G0, G1);
+                const uint32_t nr = (uint32_t)ng * kMaxTopLevels;
+                TopRun runs[kMaxTopRuns];
+                uint32_t cum[kMaxTopRuns + 1], wlo[kMaxTopRuns + 1], whi[kMaxTopRuns + 1], nw = 0;
+                cum[0] = 0;
+                for (uint32_t sl = 0; sl < nr; ++sl) {
+                    runs[sl] = btree_group_run(S, sl < kMaxTopLevels ? G0 : G1, sl % kMaxTopLevels);
+                    cum[sl + 1] = cum[sl] + runs[sl].cnt;
                 }
+                uint64_t a, bq;
+                if (btree_tile_wait(S, p0, p1, a, bq)) {
+                    wlo[nw] = (uint32_t)a;
+                    whi[nw++] = (uint32_t)bq;
+                }
+                for (uint32_t sl = 0; sl < nr; ++sl)
+                    if (runs[sl].cnt && btree_run_wait(S, runs[sl], a, bq)) {
+                        wlo[nw] = (uint32_t)a;
+                        whi[nw++] = (uint32_t)bq;
+                    }
+                for (uint32_t w = 0; w < nw; ++w)
+                    for (uint64_t kk = wlo[w]; kk <= whi[w]; ++kk) {
+                        const bool earlier = pl.bs.plan == PLAN_R ? kk >= k : kk <= k;
+                        if (!earlier || !readk[kk]) ++viol;
+                    }
+                auto covered_tile = [&](uint64_t kd) {
+                    if (kd == k) return true;
+                    for (uint32_t w = 0; w < nw; ++w)
+                        if (kd >= wlo[w] && kd <= whi[w]) return true;
+                    return false;
+                };
+                auto WD = [&](uint64_t d, uint64_t v) {  // direct store, checked against the wait list
+                    if (d >= n) { ++viol; return; }
+                    if (!covered_tile(tile_of(d))) ++viol;
+                    if (!readk[tile_of(d)]) ++viol;
+                    A[d] = v;
+                    written[d] = 1;
+                    ++pos_writes[d];
+                };
+                std::vector<uint8_t> covered(cnt, 0);
+                for (uint32_t o = 0; o < cnt; ++o) {
+                    const uint64_t x = p0 + o;
+                    uint64_t idx, ref;
+                    if (RG.kind == 0) {
+                        if (btree_is_top(S, x)) continue;
+                        if (btree_place(S, x, idx)) WD(idx, tile[o]); else SC(idx, tile[o]);
+                    } else {
+                        if (RG.kind == 2 || !btree_regime_bulk(S, RG, o, idx)) continue;
+                        const bool direct = btree_place(S, x, ref);  // fast path == reference form
+                        if (direct != RG.to_A || ref != idx) ++viol;
+                        if (RG.to_A) WD(idx, tile[o]); else SC(idx, tile[o]);
+                    }
+                    covered[o] = 1;
+                }
+                if (cum[nr] > cnt) ++viol;
+                for (uint32_t r = 0; r < nr; ++r) {
+                    if (cum[r + 1] - cum[r] != runs[r].cnt) ++viol;
+                    for (uint32_t e = 0; e < runs[r].cnt; ++e) {
+                        const uint64_t off = btree_top_item_off(S, runs[r], e);
+                        if (off >= cnt || covered[off]) { ++viol; continue; }
+                        const uint64_t p = runs[r].dest0 + e;
+                        uint64_t ref;
+                        const bool direct = btree_place(S, p0 + off, ref);
+                        if (direct != btree_run_direct(S, runs[r], e) || ref != p) ++viol;
+                        if (direct) WD(p, tile[off]); else SC(p, tile[off]);
+                        covered[off] = 1;
+                    }
+                }
+                for (uint32_t o = 0; o < cnt; ++o)
+                    if (!covered[o]) ++viol;
             } else {
                 const MvebRegion &R = P.reg[ri];
                 if (R.U == 0) {
@@ -477,17 +568,17 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
             }
         }
         if (!mv) {
-            for (uint64_t c = 0; c < pl.bs.nscratch; ++c) {
-                if (slot_writes[c] != 1) ++viol;
-                const uint64_t cc0 = c - c % kScatterChunk;
-                const ScatterDiv sd = btree_scatter_div(pl.bs, cc0);
-                const uint64_t d = btree_slot_dest(pl.bs, c);
-                if (btree_slot_dest_tile(pl.bs, sd, c) != d) ++viol;  // fast path == reference form
-                const Regime RG = btree_scatter_regime(pl.bs, cc0, std::min(pl.bs.nscratch, cc0 + kScatterChunk));
-                if (RG.kind == 1 && btree_regime_slot_dest(pl.bs, RG, cc0, (uint32_t)(c - cc0)) != d) ++viol;
-                if (d >= n) { ++viol; continue; }
-                A[d] = scr[c];
-                ++pos_writes[d];
+            for (uint64_t c = 0; c < pl.bs.nscratch; ++c)
+                if (slot_writes[c] != (btree_slot_used(pl.bs, c) ? 1u : 0u)) ++viol;
+            for (int j = 0; j < btree_copy_range_count(pl.bs); ++j) {
+                CopyRange cr;
+                if (!btree_copy_range(pl.bs, j, cr)) continue;
+                for (uint64_t e = 0; e < cr.len; ++e) {
+                    const uint64_t d = cr.dst + e, s1 = cr.src + e;
+                    if (d >= n || s1 >= pl.bs.nscratch || !btree_slot_used(pl.bs, s1)) { ++viol; continue; }
+                    A[d] = scr[s1];
+                    ++pos_writes[d];
+                }
             }
         } else {
             for (uint64_t s2 = 0; s2 < P.total_slots; ++s2) {
@@ -503,6 +594,20 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
             if (pos_writes[d] != 1) ++viol;
     }
     if (violations) *violations = viol;
+    return TL_SUCCESS;
+}
+
+// Replays the plans of both key widths (their tile sizes and scratch alignment
+// differ); the results must agree.
+int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations) {
+    std::vector<uint64_t> A4(A, A + n);
+    uint64_t v8 = 0, v4 = 0;
+    int rc = emulate_permute_kb(layout, n, b, 8, A, &v8);
+    if (!rc) rc = emulate_permute_kb(layout, n, b, 4, A4.data(), &v4);
+    if (rc) return rc;
+    uint64_t diff = 0;
+    for (uint64_t x = 0; x < n; ++x) diff += A[x] != A4[x];
+    if (violations) *violations = v8 + v4 + diff;
     return TL_SUCCESS;
 }
 

@@ -4,10 +4,10 @@
 // The in-place pass walks the array one tile at a time.  Tiles are handed out by
 // an atomic ticket counter, so a CTA holding ticket t knows every ticket below t
 // is already owned by a running CTA.  A CTA first copies its whole source tile
-// into shared memory and then publishes "tile read" (release).  Before storing,
-// it waits (acquire) for the flags of the tiles whose source overlaps the
-// destinations it will write.  Those tiles always hold smaller tickets, and a
-// CTA publishes its flag before it waits on anything, so every wait ends.  Waits
+// into shared memory and then publishes "tile read".  Before storing, it waits
+// (acquire) for the flags of the tiles whose source overlaps the destinations
+// it will write.  Those tiles always hold smaller tickets, and a CTA publishes
+// its flag before it waits on anything, so every wait ends.  Waits
 // are still bounded: on expiry the CTA records TL_ERROR_TIMEOUT in the control
 // block, skips its stores, and the host reports the error.
 #pragma once
@@ -37,8 +37,8 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
     return v;
 }
 
-__device__ __forceinline__ void st_release(unsigned int *p, unsigned int v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed(unsigned int *p, unsigned int v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // Waits until flag == want; false (and the error recorded) if the bound expires.
@@ -55,21 +55,40 @@ __device__ __forceinline__ bool wait_flag(const unsigned int *flag, unsigned int
     return false;
 }
 
-// Block-wide: fetch the next ticket (same value in every thread).
-__device__ __forceinline__ unsigned long long next_ticket(Ctrl *ctrl, unsigned long long *s_ticket) {
+// Block-wide: publish that this tile's source has been read into shared memory.
+// Every load of the tile has returned its data (cp.async.wait_all, or register
+// loads already stored to shared memory) before the barrier, so no write that
+// follows the flag can reach them: a relaxed store suffices, and thread 0 does
+// not wait for its own earlier global stores to drain as a fence would make it.
+__device__ __forceinline__ void publish_read(unsigned int *flag, const WaitCfg &wc) {
     __syncthreads();
+    if (threadIdx.x == 0) st_relaxed(flag, wc.flag_value);
+}
+
+// Block-wide ticket loop with the next ticket claimed one tile ahead: thread 0
+// issues the atomic for ticket t+1 before tile t is processed and publishes it
+// after.  A block holds at most its current and its next ticket; the current
+// tile only ever waits on smaller tickets, all of them claimed earlier, so the
+// smallest unfinished current tile always progresses.
+struct TicketPipe {
+    unsigned long long next;
+};
+
+__device__ __forceinline__ unsigned long long ticket_first(Ctrl *ctrl, unsigned long long *s_ticket) {
     if (threadIdx.x == 0) *s_ticket = atomicAdd(&ctrl->ticket, 1ull);
     __syncthreads();
     return *s_ticket;
 }
 
-// Block-wide: publish that this tile's source has been read into shared memory.
-__device__ __forceinline__ void publish_read(unsigned int *flag, const WaitCfg &wc) {
+__device__ __forceinline__ void ticket_claim(Ctrl *ctrl, TicketPipe &tp) {
+    if (threadIdx.x == 0) tp.next = atomicAdd(&ctrl->ticket, 1ull);
+}
+
+__device__ __forceinline__ unsigned long long ticket_advance(const TicketPipe &tp, unsigned long long *s_ticket) {
+    __syncthreads();  // the block is done with the current tile
+    if (threadIdx.x == 0) *s_ticket = tp.next;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        st_release(flag, wc.flag_value);
-    }
+    return *s_ticket;
 }
 
 // Block-wide: wait for tiles [k_lo, k_hi] (inclusive, global tile ids) to be read.
