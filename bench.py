@@ -417,9 +417,15 @@ def run_ours(args, rank, world, local):
             qms.append(T.query(layout, A, Q, ans, b or 16, tables=tabs, timed=True))
         hits = int((ans != n).sum().item())
         qms_med = statistics.median(qms)
+        # the binary-search comparator on the same queries over the sorted keys
+        sans = torch.empty_like(ans)
+        T.query("sorted", pristine, Q, sans)
+        sms = statistics.median([T.query("sorted", pristine, Q, sans, timed=True) for _ in range(3)])
         qinfo = {"q": q, "ms": round(qms_med, 3), "queries_per_s": round(q / (qms_med * 1e-3), 1),
-                 "hits": hits, "kernel": f"plain {layout} query"}
-        del Q, ans
+                 "hits": hits, "kernel": f"plain {layout} query",
+                 "binary_search_queries_per_s": round(q / (sms * 1e-3), 1),
+                 "binary_search_hits": int((sans != n).sum().item())}
+        del Q, ans, sans
 
     # end to end through the C ABI with host buffers: H2D keys, permute, D2H layout
     e2e = None

@@ -14,6 +14,7 @@
  *   timeQueryvEB_nonperfect<TYPE>(A, dev_A, dev_tables, dev_idx, dev_table_idx, n, d, num_tables, q)
  *                                                                        gpu/src/query-mveb.cuh:231
  *   buildTable(table, n, d, root_depth) and struct vEB_table            gpu/src/query-mveb.cu:25
+ *   timeQuery<TYPE>(A, dev_A, n, q)  (binary search, sorted dev_A)      gpu/src/binary-search.cuh:61
  *
  * Same argument meaning and return values: the permutations return host
  * wall-clock milliseconds including the final synchronisation; the queries
@@ -118,6 +119,16 @@ inline double timePermutevEB(TYPE *dev_A, uint64_t n) {
 
 inline void buildTable(vEB_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
     tl_build_table(table, n, d, root_depth);
+}
+
+template <typename TYPE>
+inline float timeQuery(TYPE *A, TYPE *dev_A, uint64_t n, uint64_t numQueries) {
+    return tree_layouts_api::query_timed(A, dev_A, n, numQueries, [&](TYPE *q, uint64_t *ans, float *ms) {
+        if (sizeof(TYPE) == 8)
+            return tl_query_sorted_u64((const uint64_t *)dev_A, n, (const uint64_t *)q, numQueries, ans, nullptr,
+                                       ms);
+        return tl_query_sorted_u32((const uint32_t *)dev_A, n, (const uint32_t *)q, numQueries, ans, nullptr, ms);
+    });
 }
 
 template <typename TYPE>

@@ -122,6 +122,15 @@ int tl_veb_tables_size(uint64_t n, uint32_t *num_tables, uint32_t *table_size, u
 int tl_build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx);
 
 /* ---------------------------------------------------------------- queries */
+/* Binary search over the sorted array (the comparator the layouts are measured
+ * against): dev_answers[i] = index of dev_queries[i] in dev_sorted, or n.
+ * Replaces searchAll / binarySearch (gpu/src/binary-search.cuh:27-57) behind
+ * timeQuery (:61-118); the reference answers a miss with its predecessor's
+ * index (and never ends for a query below A[0]; its driver issues only hits). */
+int tl_query_sorted_u32(const uint32_t *dev_sorted, uint64_t n, const uint32_t *dev_queries,
+                        uint64_t q, uint64_t *dev_answers, void *stream, float *ms);
+int tl_query_sorted_u64(const uint64_t *dev_sorted, uint64_t n, const uint64_t *dev_queries,
+                        uint64_t q, uint64_t *dev_answers, void *stream, float *ms);
 /* dev_answers[i] = position of dev_queries[i] in the layout, or n.
  * searchAll (gpu/src/query-bst.cuh:47-54) behind timeQueryBST (:58-110). */
 int tl_query_bst_u32(const uint32_t *dev_layout, uint64_t n, const uint32_t *dev_queries,

@@ -101,6 +101,20 @@ def search(layout: str, A: np.ndarray, queries: np.ndarray, b: int = 16) -> np.n
     return ans
 
 
+def search_sorted(keys: np.ndarray, queries: np.ndarray) -> np.ndarray:
+    """Binary search over the sorted keys, as binarySearch in
+    gpu/src/binary-search.cuh:27-46 does for hits (the index of the key); a miss
+    answers n here (the reference returns its predecessor's index, and does not
+    terminate for a query below keys[0])."""
+    keys = np.ascontiguousarray(keys)
+    queries = np.ascontiguousarray(queries, dtype=keys.dtype)
+    n = len(keys)
+    lb = np.searchsorted(keys, queries, side="left")
+    hit = lb < n
+    hit[hit] = keys[lb[hit]] == queries[hit]
+    return np.where(hit, lb, n).astype(np.uint64)
+
+
 def build_table(n: int, d: int) -> np.ndarray:
     t = np.zeros(max(d, 1), dtype=VEB_DTYPE)
     lib().orc_build_table(t.ctypes.data, n, d, 0)

@@ -41,6 +41,18 @@ def test_queries_match_oracle(layout, b, dtype):
         assert np.array_equal(got, exp), (layout, b, n)
 
 
+@pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
+def test_sorted_binary_search_matches_oracle(dtype):
+    for n in [1, 2, 3, 4, 5, 7, 8, 100, 4095, 4096, 8191, 8192, 8193, 65537, 1048575, 3000017]:
+        keys = data.sorted_keys_np(n, 1, 16 if dtype == np.uint64 else 3, n + 7, dtype)
+        Q = data.queries_np(keys, 5000, 0.5, n + 8)
+        edge = [keys[0] - 1 if keys[0] > 0 else keys[0], keys[0], keys[-1], keys[-1] + 1]
+        Q = np.concatenate([Q, np.array(edge, dtype=dtype)]).astype(dtype)
+        exp = O.search_sorted(keys, Q)
+        got = gpu_answers("sorted", keys, Q)
+        assert np.array_equal(got, exp), (n, dtype)
+
+
 def test_queries_match_reference_golden():
     with open(os.path.join(GOLD, "golden_cpu.json")) as f:
         g = json.load(f)

@@ -199,8 +199,7 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
                 const uint64_t a = lo > acc ? lo - acc : 0;
                 const uint64_t e = min(hi - acc, r.len);
                 if (a < e)
-                    copy_keys(keys + I.off + r.dst + a, scr + I.scr_base + r.src + a, e - a, threadIdx.x,
-                              blockDim.x);
+                    copy_keys(keys + I.off + r.dst + a, scr + I.scr_base + r.src + a, e - a, 0, 1);
                 acc += r.len;
             }
         }

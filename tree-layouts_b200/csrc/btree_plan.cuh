@@ -444,28 +444,7 @@ struct TileShared {
     uint32_t cum[kMaxTopRuns + 1];
     uint32_t nslots;
     int ok;
-    uint64_t bnd[kMaxTopLevels];  // S.bnd, for the BST pair path
 };
-
-// A leaf and the separator that follows it, from consecutive words of a tile;
-// one 16-byte (u64) or 8-byte (u32) shared-memory load when the pair is aligned.
-template <typename K>
-__device__ __forceinline__ void load_pair(const K *p, bool aligned, K &a, K &b) {
-    if (aligned) {
-        if constexpr (sizeof(K) == 8) {
-            const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
-            a = v.x;
-            b = v.y;
-        } else {
-            const uint2 v = *reinterpret_cast<const uint2 *>(p);
-            a = v.x;
-            b = v.y;
-        }
-    } else {
-        a = p[0];
-        b = p[1];
-    }
-}
 
 // Warp 0's part of btree_stream_tile: the tile's runs (one lane per slot), their
 // prefix sums, and the waits for the tiles under their direct parts.  Kept out
@@ -514,13 +493,6 @@ __device__ __forceinline__ void bar_sync_tail() {
 // computes the tile's runs of top keys (one lane per level) and waits for the
 // tiles under their direct parts, while warps 1.. wait for the tiles under the
 // bulk keys and store those; then the whole block stores the top keys.
-//
-// BST leaf tiles (b = 1, plan R) take the pair path instead: offsets 2m and
-// 2m + 1 hold leaf j and its separator, top rank j (j = p0 / 2 + m); the leaf
-// lands at ni + j, the separator on level k = ctz(j + 1) at 2^(h-1-k) - 1 +
-// ((j + 1) >> (k + 1)), directly below bnd[k] and through scratch above.  One
-// thread per pair keeps both stores coalesced across the warp and reads the
-// tile at stride 1.
 template <typename K>
 __device__ __forceinline__ bool btree_stream_tile(const BtreeStream &S, K *__restrict__ A, K *__restrict__ scr,
                                                   unsigned int *flags, Ctrl *ctrl, const WaitCfg &wc, uint64_t k,
@@ -532,61 +504,41 @@ __device__ __forceinline__ bool btree_stream_tile(const BtreeStream &S, K *__res
     publish_read(&flags[k], wc);
     const uint32_t cnt = (uint32_t)(p1 - p0);
     const K *tile = sm + (p0 - base);
-    const Regime R = btree_stream_regime(S, p0, p1);
-    const bool pairs = S.g.b == 1 && S.plan == PLAN_R && R.kind == 1;
     if (threadIdx.x < 32) {
         btree_tile_runs_warp(S, p0, p1, flags, ctrl, wc, ts);
     } else {
         const uint32_t tb = threadIdx.x - 32, nb = blockDim.x - 32;
-        if (pairs && tb < S.g.h) ts.bnd[tb] = S.bnd[tb];
         uint64_t w_lo, w_hi;
         if (btree_tile_wait(S, p0, p1, w_lo, w_hi))
             for (uint64_t f = w_lo + tb; f <= w_hi; f += nb)
                 if (!wait_flag(&flags[f], wc.wait_value, ctrl, wc)) ts.ok = 0;
-        if (!pairs) {
-            bar_sync_tail();
-            if (ts.ok) {
-                if (R.kind == 0) {
-                    for (uint64_t x = p0 + tb; x < p1; x += nb) {
-                        if (btree_is_top(S, x)) continue;
-                        uint64_t idx;
-                        const K key = sm[x - base];
-                        if (btree_place(S, x, idx))
-                            A[idx] = key;
-                        else
-                            scr[idx] = key;
-                    }
-                } else if (R.kind == 1) {
-                    K *tgt = R.to_A ? A : scr;
-                    const uint32_t d = S.fd32.d;
+        bar_sync_tail();
+        if (ts.ok) {
+            const Regime R = btree_stream_regime(S, p0, p1);
+            if (R.kind == 0) {
+                for (uint64_t x = p0 + tb; x < p1; x += nb) {
+                    if (btree_is_top(S, x)) continue;
+                    uint64_t idx;
+                    const K key = sm[x - base];
+                    if (btree_place(S, x, idx))
+                        A[idx] = key;
+                    else
+                        scr[idx] = key;
+                }
+            } else if (R.kind == 1) {
+                K *tgt = R.to_A ? A : scr;
+                const uint32_t d = S.fd32.d;
 #pragma unroll 4
-                    for (uint32_t o = tb; o < cnt; o += nb) {
-                        const uint32_t v = R.r0 + o;
-                        const uint32_t ql = S.fd32.div(v);
-                        if (v - ql * d != R.skip) tgt[R.dbase + (v - ql)] = tile[o];
-                    }
+                for (uint32_t o = tb; o < cnt; o += nb) {
+                    const uint32_t v = R.r0 + o;
+                    const uint32_t ql = S.fd32.div(v);
+                    if (v - ql * d != R.skip) tgt[R.dbase + (v - ql)] = tile[o];
                 }
             }
         }
     }
     __syncthreads();
     if (!ts.ok) return false;
-    if (pairs) {
-        const uint64_t j0 = p0 >> 1, ni = S.g.ni;
-        const uint32_t h = S.g.h;
-        const bool aligned = ((p0 - base) & 1) == 0;  // the tile buffer starts 16-byte aligned
-#pragma unroll 2
-        for (uint32_t m = threadIdx.x; m < (cnt >> 1); m += blockDim.x) {
-            K leaf, sep;
-            load_pair(tile + 2 * m, aligned, leaf, sep);
-            const uint64_t j = j0 + m, y = j + 1;
-            A[ni + j] = leaf;
-            const uint32_t lv = (uint32_t)__ffsll((long long)y) - 1;
-            const uint64_t pos = ((1ull << (h - 1 - lv)) - 1) + (y >> (lv + 1));
-            (pos < ts.bnd[lv] ? A : scr)[pos] = sep;
-        }
-        return true;
-    }
     // top keys, level by level: consecutive threads store consecutive positions
     const uint32_t total = ts.cum[ts.nslots];
     uint32_t r = 0;  // the run of gi only moves forward as gi grows
@@ -623,17 +575,20 @@ TL_HD bool btree_copy_range(const BtreeStream &S, int j, CopyRange &r) {
     return r.len != 0;
 }
 
-// Copy `len` keys src -> dst by the threads [tid, tid + nthreads) of a grid or
-// block: 16-byte vectors where src and dst share their 16-byte alignment,
-// single keys otherwise and at the ragged ends; each thread keeps 4 vectors in
-// flight.  The scratch is read once, so its loads are streaming.
-template <typename K>
+// Copy `len` keys src -> dst by the blocks [blk, blk + nblk) of a grid (or one
+// block: blk = 0, nblk = 1): 16-byte vectors where src and dst share their
+// 16-byte alignment, single keys otherwise and at the ragged ends.  The vectors
+// go in block-contiguous chunks of kUnr * blockDim: a block keeps kUnr vectors
+// per thread in flight, all from one contiguous stretch, so the DRAM rows it
+// touches stay few.  The scratch is read once, so its loads are streaming.
+template <typename K, int kUnr = 4>
 __device__ __forceinline__ void copy_keys(K *__restrict__ dst, const K *__restrict__ src, uint64_t len,
-                                          uint64_t tid, uint64_t nthreads) {
+                                          uint64_t blk, uint64_t nblk) {
     constexpr uint32_t V = 16 / sizeof(K);
+    const uint64_t tid = blk * blockDim.x + threadIdx.x;
     const uintptr_t da = reinterpret_cast<uintptr_t>(dst), sa = reinterpret_cast<uintptr_t>(src);
     if (((da ^ sa) & 15) != 0) {
-        for (uint64_t x = tid; x < len; x += nthreads) dst[x] = __ldcs(src + x);
+        for (uint64_t x = tid; x < len; x += nblk * blockDim.x) dst[x] = __ldcs(src + x);
         return;
     }
     uint64_t head = ((16 - (da & 15)) & 15) / sizeof(K);
@@ -644,15 +599,20 @@ __device__ __forceinline__ void copy_keys(K *__restrict__ dst, const K *__restri
     if (tid < len - tail0) dst[tail0 + tid] = __ldcs(src + tail0 + tid);
     uint4 *dv = reinterpret_cast<uint4 *>(dst + head);
     const uint4 *sv = reinterpret_cast<const uint4 *>(src + head);
-    uint64_t v = tid;
-    for (; v + 3 * nthreads < nvec; v += 4 * nthreads) {
-        uint4 a[4];
+    const uint64_t chunk = (uint64_t)kUnr * blockDim.x;
+    for (uint64_t c0 = blk * chunk; c0 < nvec; c0 += nblk * chunk) {
+        uint4 a[kUnr];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) a[u] = __ldcs(sv + v + u * nthreads);
+        for (int u = 0; u < kUnr; ++u) {
+            const uint64_t v = c0 + u * blockDim.x + threadIdx.x;
+            if (v < nvec) a[u] = __ldcs(sv + v);
+        }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) dv[v + u * nthreads] = a[u];
+        for (int u = 0; u < kUnr; ++u) {
+            const uint64_t v = c0 + u * blockDim.x + threadIdx.x;
+            if (v < nvec) dv[v] = a[u];
+        }
     }
-    for (; v < nvec; v += nthreads) dv[v] = __ldcs(sv + v);
 }
 
 }  // namespace tl

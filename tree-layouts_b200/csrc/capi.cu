@@ -280,6 +280,12 @@ int tl_query_btree_learned_u64(const uint64_t *A, uint64_t n, uint64_t b, const 
         return query(a, S(stream), ms);                                                                 \
     }
 
+TL_Q(tl_query_sorted_u32(const uint32_t *L, uint64_t n, const uint32_t *Q, uint64_t q, uint64_t *ans,
+                         void *stream, float *ms),
+     uint32_t, 4, Q_SORTED, a.layout_keys = L; a.n = n; a.queries = Q; a.q = q; a.answers = ans)
+TL_Q(tl_query_sorted_u64(const uint64_t *L, uint64_t n, const uint64_t *Q, uint64_t q, uint64_t *ans,
+                         void *stream, float *ms),
+     uint64_t, 8, Q_SORTED, a.layout_keys = L; a.n = n; a.queries = Q; a.q = q; a.answers = ans)
 TL_Q(tl_query_bst_u32(const uint32_t *L, uint64_t n, const uint32_t *Q, uint64_t q, uint64_t *ans, void *stream,
                       float *ms),
      uint32_t, 4, Q_BST, a.layout_keys = L; a.n = n; a.queries = Q; a.q = q; a.answers = ans)

@@ -87,7 +87,7 @@ int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *v
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
             uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms = nullptr);
 
-enum QueryLayout { Q_BST = 0, Q_BTREE = 1, Q_VEB = 2, Q_VEB_NP = 3 };
+enum QueryLayout { Q_BST = 0, Q_BTREE = 1, Q_VEB = 2, Q_VEB_NP = 3, Q_SORTED = 4 };
 struct QueryArgs {
     int layout;
     uint32_t key_bytes;

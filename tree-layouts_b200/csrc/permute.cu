@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "btree_plan.cuh"
+#include "bulk.cuh"
 #include "geometry.cuh"
 #include "internal.h"
 #include "stream.cuh"
@@ -58,16 +59,45 @@ btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constan
 }
 
 // Second pass of a B-tree permutation: the scratch ranges to their final
-// positions, a plain copy (scratch is indexed by final position).
+// positions, a plain copy (scratch is indexed by final position) through the
+// bulk-copy engine.
 template <typename K>
-__global__ void __launch_bounds__(kScatterThreads)
-btree_copy_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_constant__ BtreeStream S) {
-    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
-    const int nr = btree_copy_range_count(S);
-    for (int j = 0; j < nr; ++j) {
+__global__ void __launch_bounds__(32)
+btree_copy_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_constant__ BulkPlan P, Ctrl *ctrl) {
+    extern __shared__ __align__(128) unsigned char stage[];
+    __shared__ __align__(8) uint64_t bars[kBulkStages];
+    bulk_copy_plan(A, scr, P, stage, bars, ctrl);
+}
+
+// The copy ranges split for the bulk engine: each range's 16-byte-aligned
+// interior in kBulkChunk pieces, its ragged keys apart.  The scratch shares A's
+// offset within 16 bytes at both range bases, so the interiors line up.
+template <typename K>
+static int make_bulk_plan(const BtreeStream &S, const K *A, const K *scr, BulkPlan &P) {
+    P.nr = 0;
+    P.nchunks = 0;
+    for (int j = 0; j < btree_copy_range_count(S); ++j) {
         CopyRange r;
-        if (btree_copy_range(S, j, r)) copy_keys(A + r.dst, scr + r.src, r.len, tid, nth);
+        if (!btree_copy_range(S, j, r)) continue;
+        if (P.nr == kMaxBulkRanges) return TL_ERROR_UNSUPPORTED;
+        const uintptr_t da = reinterpret_cast<uintptr_t>(A + r.dst), sa = reinterpret_cast<uintptr_t>(scr + r.src);
+        if ((da ^ sa) & 15) return TL_ERROR_INVALID_VALUE;
+        BulkRange R{};
+        R.key_dst = r.dst;
+        R.key_src = r.src;
+        R.len = r.len;
+        const uint64_t head = std::min<uint64_t>(((16 - (da & 15)) & 15) / sizeof(K), r.len);
+        const uint64_t body = ((r.len - head) * sizeof(K)) & ~15ull;
+        R.head = (uint32_t)head;
+        R.tail = (uint32_t)(r.len - head - body / sizeof(K));
+        R.dst = (r.dst + head) * sizeof(K);
+        R.src = (r.src + head) * sizeof(K);
+        R.bytes = body;
+        R.chunk0 = P.nchunks;
+        P.nchunks += (body + kBulkChunk - 1) / kBulkChunk;
+        P.r[P.nr++] = R;
     }
+    return TL_SUCCESS;
 }
 
 // ---------------------------------------------------------------- mvEB stream
@@ -317,15 +347,18 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, wc, flags);
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
-        if (pl.scratch_keys) {
-            // resident blocks striding over the copy, 4 vectors in flight per thread
+        BulkPlan bp;
+        int rc = make_bulk_plan(pl.bs, A, scr, bp);
+        if (rc) return rc;
+        if (bp.nr) {
+            // one warp per CTA, as many CTAs per SM as the stages' shared memory allows
+            const size_t smem = (size_t)kBulkStages * kBulkChunk;
+            auto ck = btree_copy_kernel<K>;
+            TL_CUDA_TRY(cudaFuncSetAttribute(ck, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int cper = 0;
-            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cper, btree_copy_kernel<K>,
-                                                                      kScatterThreads, 0));
-            const uint64_t per_block = (uint64_t)kScatterThreads * 4 * (16 / sizeof(K));
-            uint64_t cg = std::min<uint64_t>((pl.scratch_keys + per_block - 1) / per_block,
-                                             (uint64_t)std::max(cper, 1) * smx);
-            btree_copy_kernel<K><<<(unsigned)std::max<uint64_t>(cg, 1), kScatterThreads, 0, st>>>(A, scr, pl.bs);
+            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cper, ck, 32, smem));
+            const uint64_t cg = std::max<uint64_t>(1, std::min<uint64_t>(bp.nchunks, (uint64_t)std::max(cper, 1) * smx));
+            ck<<<(unsigned)cg, 32, smem, st>>>(A, scr, bp, ctrl);
             TL_CUDA_TRY(cudaGetLastError());
         }
     }

@@ -55,6 +55,59 @@ bst_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, const K *__res
     }
 }
 
+// ---------------------------------------------------------------- sorted array
+// The binary-search comparator (gpu/src/binary-search.cuh:27-57 searches the
+// sorted array before any permutation).  Branch-free lower bound: with
+// len_0 = n and base_0 = 0, step d probes base_d + half_d (half_d = len_d / 2),
+// base_{d+1} = base_d + half_d when that key is below the query, len_{d+1} =
+// len_d - half_d; then the answer is the lower bound if it holds the query,
+// else n.  The lengths do not depend on the query, so the keys probed in the
+// first L steps form a complete binary tree of 2^L - 1 positions; they are
+// pinned in shared memory in breadth-first order (node i has children 2i and
+// 2i + 1, path bit = "went right"), which turns those steps into
+// shared-memory loads.
+template <typename K>
+__global__ void __launch_bounds__(kQueryThreads)
+sorted_query_kernel(const K *__restrict__ A, uint64_t n, uint32_t L, const K *__restrict__ Q, uint64_t nq,
+                    uint64_t *__restrict__ ans) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *tree = reinterpret_cast<K *>(smem_raw);  // tree[1 .. 2^L - 1]
+    const uint32_t nodes = (1u << L) - 1;
+    for (uint32_t node = threadIdx.x + 1; node <= nodes; node += blockDim.x) {
+        // replay the path of `node`: its bits below the leading one, high to low
+        const uint32_t depth = 31 - __clz(node);
+        uint64_t base = 0, len = n;
+        for (uint32_t d = 0; d < depth; ++d) {
+            const uint64_t half = len >> 1;
+            if ((node >> (depth - 1 - d)) & 1u) base += half;
+            len -= half;
+        }
+        tree[node] = __ldg(A + base + (len >> 1));
+    }
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
+        const K q = __ldcs(Q + qi);
+        uint64_t base = 0, len = n;
+        uint32_t node = 1;
+        for (uint32_t d = 0; d < L; ++d) {  // len > 1 throughout: L < log2(n)
+            const uint64_t half = len >> 1;
+            const bool right = tree[node] < q;
+            base += right ? half : 0;
+            len -= half;
+            node = 2 * node + right;
+        }
+        while (len > 1) {
+            const uint64_t half = len >> 1;
+            base += __ldg(A + base + half) < q ? half : 0;
+            len -= half;
+        }
+        const K at = __ldg(A + base);
+        const uint64_t lb = base + (at < q);
+        __stcs(ans + qi, (lb < n && (lb == base ? at : __ldg(A + lb)) == q) ? lb : n);
+    }
+}
+
 // ---------------------------------------------------------------- B-tree
 // searchBtree (cpu/src/query-btree.h:33-54): the child followed is the number of
 // node keys smaller than the query; an equal key ends the search.  A group of G
@@ -287,7 +340,17 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
     const K *Q = static_cast<const K *>(a.queries);
     uint64_t P = std::min<uint64_t>(a.n, kPinBytes / sizeof(K));
     unsigned grid = 1;
-    if (a.layout == Q_BST) {
+    if (a.layout == Q_SORTED) {
+        // pinned probe tree: L levels with 2^L - 1 < n (so every pinned step has
+        // len > 1) and at most 32 KB of keys
+        uint32_t L = 0;
+        while (L < 12 && ((2ull << L) - 1) * sizeof(K) <= 32768 && (2ull << L) <= a.n) ++L;
+        const size_t smem = ((size_t)1 << L) * sizeof(K);
+        auto kern = sorted_query_kernel<K>;
+        int rc = persistent_grid(kern, smem, a.q, &grid);
+        if (rc) return rc;
+        kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, L, Q, a.q, a.answers);
+    } else if (a.layout == Q_BST) {
         // whole top levels: 2^T - 1 keys
         uint64_t top = 1;
         while (top * 2 + 1 <= P) top = top * 2 + 1;

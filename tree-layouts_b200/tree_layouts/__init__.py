@@ -68,6 +68,7 @@ def lib():
         L.tl_build_veb_tables.argtypes = [_u64, _v, _v, _v]
         for w in ("u32", "u64"):
             getattr(L, f"tl_query_bst_{w}").argtypes = [_v, _u64, _v, _u64, _v, _v, _f32p]
+            getattr(L, f"tl_query_sorted_{w}").argtypes = [_v, _u64, _v, _u64, _v, _v, _f32p]
             getattr(L, f"tl_query_btree_{w}").argtypes = [_v, _u64, _u64, _v, _u64, _v, _v, _f32p]
             getattr(L, f"tl_query_veb_{w}").argtypes = [_v, _v, _u64, _u32, _v, _u64, _v, _v, _f32p]
             getattr(L, f"tl_query_veb_nonperfect_{w}").argtypes = [_v, _v, _v, _v, _u64, _u32, _u32, _v,
@@ -175,7 +176,8 @@ class VebTablesDevice:
 
 def query(layout: str, tree, queries, answers, b: int = 16, tables: VebTablesDevice | None = None,
           stream=None, timed: bool = False):
-    """answers[i] = position of queries[i] in the layout `tree`, or n."""
+    """answers[i] = position of queries[i] in the layout `tree`, or n.  Layout
+    "sorted": binary search over the sorted (unpermuted) keys."""
     L = lib()
     w = "u64" if _key_bytes(tree) == 8 else "u32"
     assert queries.element_size() == tree.element_size()
@@ -183,8 +185,9 @@ def query(layout: str, tree, queries, answers, b: int = 16, tables: VebTablesDev
     ms = C.c_float(0.0)
     msp = C.byref(ms) if timed else None
     s = _stream_ptr(stream)
-    if layout == "bst":
-        rc = getattr(L, f"tl_query_bst_{w}")(tree.data_ptr(), n, queries.data_ptr(), q, answers.data_ptr(), s, msp)
+    if layout in ("bst", "sorted"):
+        rc = getattr(L, f"tl_query_{layout}_{w}")(tree.data_ptr(), n, queries.data_ptr(), q, answers.data_ptr(), s,
+                                                   msp)
     elif layout == "btree":
         rc = getattr(L, f"tl_query_btree_{w}")(tree.data_ptr(), n, b, queries.data_ptr(), q, answers.data_ptr(),
                                                s, msp)
