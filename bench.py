@@ -253,8 +253,8 @@ def learned_section(args, dev):
     used = lv["empty"] == 0
     win = (lv["eps_lo"].astype(np.int64) + lv["eps_hi"])[used]
     pm, lm = statistics.median(p_ms), statistics.median(l_ms)
-    out = {"workload": "btree-b16-n2^30-u64 skewed keys (lognormal sigma=2 + 5% in 1000 clusters), "
-                       "2^28 queries 90% Zipf(1.1) / 10% uniform misses",
+    out = {"workload": f"B-tree b=16 over n={n} skewed u64 keys (lognormal sigma=2 + 5% in 1000 clusters), "
+                       f"{q} queries 90% Zipf(1.1) / 10% uniform misses",
            "n": n, "q": q, "plain_queries_per_s": round(q / (pm * 1e-3), 1),
            "learned_queries_per_s": round(q / (lm * 1e-3), 1), "speedup": round(pm / lm, 3),
            "exact": exact, "plain_ms": round(pm, 3), "learned_ms": round(lm, 3),
@@ -324,8 +324,8 @@ def batched_section(args, dev):
     qms = statistics.median(plan.query(keys, Q, inst, ans, timed=True) for _ in range(3))
     del g
     pm = statistics.median(ms)
-    out = {"workload": "4096 uint64 arrays, sizes log-uniform [2^10, 2^22], b = 8, one persistent launch "
-                       "replayed from a CUDA graph; 2^26 queries, 70% hits",
+    out = {"workload": f"{len(sizes)} uint64 arrays, sizes log-uniform [2^10, 2^22], b = 8, one persistent launch "
+                       f"replayed from a CUDA graph; {args.batch_q} queries, 70% hits",
            "arrays": len(sizes), "total_keys": total,
            "permute_ms": round(pm, 3), "permute_GBps": round(2.0 * total * 8 / (pm * 1e-3) / 1e9, 1),
            "permute_frac_of_peak": round(2.0 * total * 8 / (pm * 1e-3) / 1e9 / peaks()[0], 4),

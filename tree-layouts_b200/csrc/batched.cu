@@ -162,6 +162,8 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
     __shared__ __align__(16) unsigned char s_inst_raw[sizeof(BatchInst)];
     __shared__ TileShared ts;
     const BatchInst &I = *reinterpret_cast<const BatchInst *>(s_inst_raw);
+    __shared__ uint32_t s_loaded;  // instance whose plan s_inst_raw holds
+    if (threadIdx.x == 0) s_loaded = 0xFFFFFFFFu;
     TicketPipe tp;
     for (unsigned long long t = ticket_first(ctrl, &s_ticket); t < tot.tiles + tot.chunks;
          t = ticket_advance(tp, &s_ticket)) {
@@ -173,12 +175,13 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
             if (!is_tile) s_ok = wait_flag(&done[s_j], (unsigned int)inst[s_j].S.ntiles, ctrl, wc) ? 1 : 0;
         }
         __syncthreads();
-        {  // the owner's plan into shared memory: every thread reads it many times
+        if (s_j != s_loaded) {  // the owner's plan into shared memory: every thread reads it many times
             const uint4 *src = reinterpret_cast<const uint4 *>(inst + s_j);
             uint4 *dst = reinterpret_cast<uint4 *>(s_inst_raw);
             for (uint32_t w = threadIdx.x; w < sizeof(BatchInst) / 16; w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            if (threadIdx.x == 0) s_loaded = s_j;
         }
-        __syncthreads();
         if (!s_ok) continue;
         if (is_tile) {
             const uint64_t k = btree_tile_of_ticket(I.S, t - I.tile_base);

@@ -185,6 +185,7 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
             for (uint32_t q = threadIdx.x; q < (1u << R.U) - 1; q += blockDim.x) s_inv[q] = src[q];
             loaded_U = R.U;
         }
+        if (threadIdx.x == 0) s_ok = 1;  // the previous tile's readers are past the ticket barrier
         const uint64_t base = load_tile(A, p0, p1, sm);
         publish_read(&flags[k], wc);
         if (R.U == 0) {
@@ -193,9 +194,12 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
             continue;
         }
         uint64_t k_lo, k_hi;
-        if (mveb_tile_wait(P, R, p0, p1, k_lo, k_hi) &&
-            !wait_tiles(flags, (long long)k_lo, (long long)k_hi, ctrl, wc, &s_ok))
-            continue;
+        if (mveb_tile_wait(P, R, p0, p1, k_lo, k_hi)) {
+            for (uint64_t f = k_lo + threadIdx.x; f <= k_hi; f += blockDim.x)
+                if (!wait_flag(&flags[f], wc.wait_value, ctrl, wc)) s_ok = 0;
+            __syncthreads();
+            if (!s_ok) continue;
+        }
         const uint32_t U = R.U;
         const uint64_t u = (1ull << U) - 1;
         uint64_t g0, g1;

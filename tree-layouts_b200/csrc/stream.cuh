@@ -91,18 +91,6 @@ __device__ __forceinline__ unsigned long long ticket_advance(const TicketPipe &t
     return *s_ticket;
 }
 
-// Block-wide: wait for tiles [k_lo, k_hi] (inclusive, global tile ids) to be read.
-// Returns true when all were seen before the bound expired.
-__device__ __forceinline__ bool wait_tiles(const unsigned int *flags, long long k_lo, long long k_hi,
-                                           Ctrl *ctrl, const WaitCfg &wc, int *s_ok) {
-    if (threadIdx.x == 0) *s_ok = 1;
-    __syncthreads();
-    for (long long k = k_lo + threadIdx.x; k <= k_hi; k += blockDim.x)
-        if (!wait_flag(&flags[k], wc.wait_value, ctrl, wc)) *s_ok = 0;
-    __syncthreads();
-    return *s_ok != 0;
-}
-
 // Copies src[p0, p1) into shared memory so that element x sits at
 // sm[x - base], base = p0 rounded down to a 16-byte boundary of the global
 // address.  Returns base when the copy has landed.  The 16-byte-aligned interior
