@@ -36,6 +36,9 @@ WORKLOADS = {
     "btree-b16-n2^30-u64": ("btree", 16, 2**30, 8, 16, 8, 2**27, 9),
     "mveb-n2^30-1-u32": ("mveb", 0, 2**30 - 1, 4, 3, 5, 2**27, 6),
     "mveb-n300M-u32": ("mveb", 0, 300_000_000, 4, 3, 5, 2**27, 6),
+    # the standard vEB layout of the reference's CPU code
+    "veb-n2^30-1-u32": ("veb", 0, 2**30 - 1, 4, 3, 5, 2**27, 6),
+    "veb-n300M-u32": ("veb", 0, 300_000_000, 4, 3, 5, 2**27, 6),
     "bst-n2^30-1-u64": ("bst", 1, 2**30 - 1, 8, 16, 1, 2**27, 2),
     "bst-n2^20-1-u64": ("bst", 1, 2**20 - 1, 8, 16, 1, 2**20, 2),
     # small cases for ncu captures (inputs above L2, a few GB on the device)
@@ -139,15 +142,16 @@ class ClockSampler:
 
 
 REF_FUNCS = {"bst": "timePermuteBST (cpu/src/bst-involutions.h)",
-             "btree": "timePermuteBtree (cpu/src/btree-cycles.h)"}
+             "btree": "timePermuteBtree (cpu/src/btree-cycles.h)",
+             "veb": "timePermutevEB (cpu/src/veb-cycles.h)"}
 
 
 def cpu_reference_permute(layout, b, n_sample, key_bytes, reps, min_seconds=8.0):
     """The reference's own CPU OpenMP permutation (compiled from its sources into
-    oracle/_ref/libref_cpu.so) on n_sample uint64 keys with every host thread.
-    The reference has no CPU mvEB (its CPU tree is the standard vEB), and the
-    oracle's single-thread C restatement of its mvEB stands in there, as it does
-    for every layout when that build is absent."""
+    oracle/_ref/libref_cpu.so: B-tree, BST, standard vEB) on n_sample uint64 keys
+    with every host thread.  The reference has no CPU mvEB (its CPU tree is the
+    standard vEB), and the oracle's single-thread C restatement of its mvEB
+    stands in there, as it does for every layout when that build is absent."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -164,11 +168,13 @@ def cpu_reference_permute(layout, b, n_sample, key_bytes, reps, min_seconds=8.0)
         if ref is not None:
             if layout == "bst":
                 ms = ref.ref_cpu_permute_bst_u64(A, n_sample, threads)
+            elif layout == "veb":
+                ms = ref.ref_cpu_permute_veb_u64(A, n_sample, threads)
             else:
                 ms = ref.ref_cpu_permute_btree_u64(A, n_sample, b, threads)
-        elif layout == "mveb":
+        elif layout in ("mveb", "veb"):
             t0 = time.perf_counter()
-            O.lib().orc_permute_mveb(A, n_sample)
+            (O.lib().orc_permute_mveb if layout == "mveb" else O.lib().orc_permute_veb_std)(A, n_sample)
             ms = (time.perf_counter() - t0) * 1e3
         else:
             ms = O.lib().orc_time_permute_btree(A, n_sample, b if layout != "bst" else 1)
@@ -409,7 +415,7 @@ def run_ours(args, rank, world, local):
     if args.queries and q:
         Q = data.queries_torch(pristine, q, 0.5, qseed)
         ans = torch.empty(q, dtype=torch.int64, device=dev)
-        tabs = T.VebTablesDevice(n, dev) if layout == "mveb" else None
+        tabs = T.VebTablesDevice(n, dev, standard=layout == "veb") if layout in ("mveb", "veb") else None
         for _ in range(2):
             T.query(layout, A, Q, ans, b or 16, tables=tabs)
         qms = []
@@ -479,12 +485,12 @@ def run_ours(args, rank, world, local):
                        "l2": "inputs larger than L2 (no flush needed)",
                        "restore": "array re-initialised from a pristine copy between steps, untimed",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
-            "roofline": {"bound": "hbm", "kernel": "mveb_stream_kernel" if layout == "mveb" else "btree_stream_kernel",
+            "roofline": {"bound": "hbm", "kernel": "mveb_stream_kernel" if layout in ("mveb", "veb") else "btree_stream_kernel",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": f"hbm_gbs of {peak_kind}",
                          "traffic": traffic, "algorithmic_bytes_per_launch": int(bytes_step),
                          "stream_ms": round(stream_ms, 4),
-                         "pass2_kernel": "mveb_scatter_kernel" if layout == "mveb" else "btree_copy_kernel",
+                         "pass2_kernel": "mveb_scatter_kernel" if layout in ("mveb", "veb") else "btree_copy_kernel",
                          "pass2_ms": round(pass2_ms, 4), "pass2_bytes_per_launch": int(pass2_bytes),
                          "pass2_achieved": round(pass2_bytes / (pass2_ms * 1e-3) / 1e9, 1) if pass2_ms > 0 else None,
                          "whole_permute_frac": round(bytes_step / (ms_local * 1e-3) / 1e9 / peak, 4)},

@@ -49,7 +49,8 @@ typedef enum tl_status {
 typedef enum tl_layout {
     TL_LAYOUT_BST = 0,
     TL_LAYOUT_BTREE = 1,
-    TL_LAYOUT_MVEB = 2
+    TL_LAYOUT_MVEB = 2,
+    TL_LAYOUT_VEB = 3  /* the standard van Emde Boas layout of the reference's CPU code */
 } tl_layout;
 
 /* Brodal-Fagerberg-Jacob position table; same layout (24 bytes) as the
@@ -93,6 +94,12 @@ int tl_permute_btree_u64(uint64_t *dev_A, uint64_t n, uint64_t b, void *stream, 
 /* timePermutevEB<TYPE>(TYPE *dev_A, uint64_t n): gpu/src/mveb-cycles.cuh:420 */
 int tl_permute_mveb_u32(uint32_t *dev_A, uint64_t n, void *stream, float *ms);
 int tl_permute_mveb_u64(uint64_t *dev_A, uint64_t n, void *stream, float *ms);
+/* The standard van Emde Boas layout (root floor(d/2), bottoms ceil(d/2) levels),
+ * which the reference builds on the CPU only: timePermutevEB<TYPE>(TYPE *A,
+ * uint64_t n, uint32_t p), cpu/src/veb-cycles.h:380-395.  Here on the device,
+ * in place, as tl_permute(TL_LAYOUT_VEB, ...). */
+int tl_permute_veb_std_u32(uint32_t *dev_A, uint64_t n, void *stream, float *ms);
+int tl_permute_veb_std_u64(uint64_t *dev_A, uint64_t n, void *stream, float *ms);
 
 /* No counterpart in the reference.  tl_permute for callers that cannot allocate
  * device memory (a plugin inside a host engine that owns every allocation, a
@@ -120,6 +127,15 @@ int tl_veb_tables_size(uint64_t n, uint32_t *num_tables, uint32_t *table_size, u
 /* Fills tables[table_size] (zeroed here), idx[num_tables], table_idx[num_tables]
  * exactly as gpu/test/query-mveb-fixedN.cu:130-165 builds them. */
 int tl_build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx);
+/* The same three for the standard vEB layout: buildTable of
+ * cpu/src/query-veb.cpp:25-41, and the table set of the reference's CPU query
+ * driver cpu/test/query-veb-fixedN.cpp:37-150 (one table per division, here
+ * concatenated with table_idx offsets).  tl_query_veb_* and
+ * tl_query_veb_nonperfect_* answer queries over a standard vEB layout given
+ * these tables (the descent of cpu/src/query-veb.h:41-64 is the same). */
+void tl_build_table_std(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth);
+int tl_veb_tables_size_std(uint64_t n, uint32_t *num_tables, uint32_t *table_size, uint32_t *d);
+int tl_build_veb_tables_std(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx);
 
 /* ---------------------------------------------------------------- queries */
 /* Binary search over the sorted array (the comparator the layouts are measured

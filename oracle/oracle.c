@@ -327,6 +327,145 @@ int orc_permute_mveb(uint64_t *A, uint64_t n) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* Standard van Emde Boas layout of the reference's CPU code                  */
+/* ------------------------------------------------------------------------ */
+
+/* cpu/src/veb-cycles.h:118-119: root_d = floor((d - 2)/2) + 1, leaf_d = the rest. */
+static void veb_std_split(uint32_t d, uint32_t *root_d, uint32_t *leaf_d) {
+    *root_d = (d - 2) / 2 + 1;
+    *leaf_d = d - *root_d;
+}
+
+/* permutevEB: cpu/src/veb-cycles.h:33-57.  equidistant_gather_io (cpu/src/cycles.h:
+ * 89-141) performs the cycles of equidistant_gather b at a time; the resulting
+ * permutation is the same. */
+static void permute_veb_std(uint64_t *A, uint64_t n, uint32_t d) {
+    if (d <= 1) return;
+    if (d % 2 == 0) {
+        uint64_t m = ((uint64_t)1 << (d / 2)) - 1;
+        equidistant_gather(A, m, m);
+        for (uint64_t i = 0; i < n; i += m) permute_veb_std(&A[i], m, d / 2);
+    } else {
+        uint64_t r = ((uint64_t)1 << (d / 2)) - 1;
+        uint64_t l = 2 * r + 1;
+        equidistant_gather(A, r, l);
+        permute_veb_std(A, r, d / 2);
+        for (uint64_t i = r; i < n; i += l) permute_veb_std(&A[i], l, d / 2 + 1);
+    }
+}
+
+/* permutevEB_nonperfect: cpu/src/veb-cycles.h:111-173 (2^(d-1) - 1 < n < 2^d - 1). */
+static void permute_veb_std_nonperfect(uint64_t *A, uint64_t n, uint32_t d) {
+    if (d <= 1) return;
+    uint32_t root_d, leaf_d;
+    veb_std_split(d, &root_d, &leaf_d);
+    uint64_t r = ((uint64_t)1 << root_d) - 1;
+    uint64_t l = ((uint64_t)1 << leaf_d) - 1;
+    uint64_t num_full = (n - r) / l;
+    uint64_t inc_n = n - r - num_full * l;
+    equidistant_gather(A, num_full, l);
+    if (num_full < r) shift_right(&A[num_full], n - num_full, r - num_full);
+    uint64_t size;
+    if (root_d == leaf_d) {
+        size = (num_full + 1) * r;
+        for (uint64_t i = 0; i < size; i += r) permute_veb_std(&A[i], r, root_d);
+    } else {
+        permute_veb_std(A, r, root_d);
+        size = r + num_full * l;
+        for (uint64_t i = r; i < size; i += l) permute_veb_std(&A[i], l, leaf_d);
+    }
+    if (inc_n > 0) {
+        uint32_t inc_d = bit_length(inc_n);
+        if (inc_n != ((uint64_t)1 << inc_d) - 1)
+            permute_veb_std_nonperfect(&A[size], inc_n, inc_d);
+        else
+            permute_veb_std(&A[size], inc_n, inc_d);
+    }
+}
+
+/* timePermutevEB: cpu/src/veb-cycles.h:380-395 (h = log2(n), d = h + 1 = the bit
+ * length of n below 2^52). */
+int orc_permute_veb_std(uint64_t *A, uint64_t n) {
+    if (n == 0) return 0;
+    uint32_t d = bit_length(n);
+    if (n != ((uint64_t)1 << d) - 1)
+        permute_veb_std_nonperfect(A, n, d);
+    else
+        permute_veb_std(A, n, d);
+    return 0;
+}
+
+/* buildTable: cpu/src/query-veb.cpp:25-41 (standard split). */
+void orc_build_table_std(orc_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
+    if (n == 1) return;
+    uint32_t root_d, leaf_d;
+    veb_std_split(d, &root_d, &leaf_d);
+    uint64_t root_n = ((uint64_t)1 << root_d) - 1;
+    uint64_t leaf_n = ((uint64_t)1 << leaf_d) - 1;
+    uint32_t i = d - leaf_d;
+    table[i].L = leaf_n;
+    table[i].R = root_n;
+    table[i].D = root_depth;
+    orc_build_table_std(table, root_n, root_d, root_depth);
+    orc_build_table_std(&table[i], leaf_n, leaf_d, i + root_depth);
+}
+
+/* Table-set sizing of cpu/test/query-veb-fixedN.cpp:37-84 (standard split). */
+void orc_veb_tables_size_std(uint64_t n, uint32_t *num_tables, uint32_t *table_size) {
+    uint32_t d = bit_length(n);
+    uint32_t nt = 1, ts = d;
+    if (n != ((uint64_t)1 << d) - 1) {
+        uint64_t temp_n = n;
+        uint32_t temp_d = d;
+        while (temp_d >= 2) {
+            uint32_t root_d, leaf_d;
+            veb_std_split(temp_d, &root_d, &leaf_d);
+            uint64_t r = ((uint64_t)1 << root_d) - 1;
+            uint64_t l = ((uint64_t)1 << leaf_d) - 1;
+            uint64_t num_full = (temp_n - r) / l;
+            uint64_t inc_n = temp_n - r - num_full * l;
+            if (inc_n == 0) break;
+            uint32_t inc_d = bit_length(inc_n);
+            ++nt;
+            ts += inc_d;
+            temp_n = inc_n;
+            temp_d = inc_d;
+            if (temp_n == ((uint64_t)1 << inc_d) - 1) break;
+        }
+    }
+    *num_tables = nt;
+    *table_size = ts;
+}
+
+/* Table-set construction of cpu/test/query-veb-fixedN.cpp:120-150, the tables
+ * concatenated as the GPU driver lays them out (table_idx offsets). */
+void orc_build_veb_tables_std(uint64_t n, orc_veb_table *tables, uint64_t *idx, uint32_t *table_idx) {
+    uint32_t num_tables, table_size;
+    orc_veb_tables_size_std(n, &num_tables, &table_size);
+    memset(tables, 0, table_size * sizeof(orc_veb_table));
+    uint32_t d = bit_length(n);
+    orc_build_table_std(tables, n, d, 0);
+    idx[num_tables - 1] = n;
+    table_idx[0] = 0;
+    uint64_t temp_n = n;
+    uint32_t temp_d = d;
+    for (uint32_t i = 1; i < num_tables; ++i) {
+        table_idx[i] = table_idx[i - 1] + temp_d;
+        uint32_t root_d, leaf_d;
+        veb_std_split(temp_d, &root_d, &leaf_d);
+        uint64_t r = ((uint64_t)1 << root_d) - 1;
+        uint64_t l = ((uint64_t)1 << leaf_d) - 1;
+        uint64_t num_full = (temp_n - r) / l;
+        uint64_t inc_n = temp_n - r - num_full * l;
+        uint32_t inc_d = bit_length(inc_n);
+        orc_build_table_std(&tables[table_idx[i]], inc_n, inc_d, 0);
+        idx[i - 1] = n - inc_n;
+        temp_n = inc_n;
+        temp_d = inc_d;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Queries                                                                    */
 /* ------------------------------------------------------------------------ */
 

@@ -30,6 +30,8 @@ extern "C" {
 int orc_permute_btree(uint64_t *A, uint64_t n, uint64_t b);
 int orc_permute_bst(uint64_t *A, uint64_t n);
 int orc_permute_mveb(uint64_t *A, uint64_t n);
+/* the standard vEB of the reference's CPU code (cpu/src/veb-cycles.h) */
+int orc_permute_veb_std(uint64_t *A, uint64_t n);
 
 /* Point queries: ans[i] = position of q[i] in the layout, or n if absent.
  * Keys are compared as unsigned 64-bit integers (pass 32-bit keys widened). */
@@ -49,6 +51,9 @@ void orc_build_table(orc_veb_table *table, uint64_t n, uint32_t d, uint32_t root
 void orc_veb_tables_size(uint64_t n, uint32_t *num_tables, uint32_t *table_size);
 /* Fills tables[table_size], idx[num_tables], table_idx[num_tables]. */
 void orc_build_veb_tables(uint64_t n, orc_veb_table *tables, uint64_t *idx, uint32_t *table_idx);
+void orc_build_table_std(orc_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth);
+void orc_veb_tables_size_std(uint64_t n, uint32_t *num_tables, uint32_t *table_size);
+void orc_build_veb_tables_std(uint64_t n, orc_veb_table *tables, uint64_t *idx, uint32_t *table_idx);
 void orc_search_veb(const uint64_t *A, const orc_veb_table *table, uint64_t n, uint32_t d,
                     const uint64_t *q, uint64_t nq, uint64_t *ans);
 void orc_search_veb_nonperfect(const uint64_t *A, const orc_veb_table *tables, const uint64_t *idx,

@@ -44,6 +44,10 @@ def lib():
         L.orc_permute_btree.argtypes = [_u64p, C.c_uint64, C.c_uint64]
         L.orc_permute_bst.argtypes = [_u64p, C.c_uint64]
         L.orc_permute_mveb.argtypes = [_u64p, C.c_uint64]
+        L.orc_permute_veb_std.argtypes = [_u64p, C.c_uint64]
+        L.orc_build_table_std.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32]
+        L.orc_veb_tables_size_std.argtypes = [C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.orc_build_veb_tables_std.argtypes = [C.c_uint64, C.c_void_p, _u64p, _u32p]
         L.orc_search_bst.argtypes = [_u64p, C.c_uint64, _u64p, C.c_uint64, _u64p]
         L.orc_search_btree.argtypes = [_u64p, C.c_uint64, C.c_uint64, _u64p, C.c_uint64, _u64p]
         L.orc_build_table.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32]
@@ -69,6 +73,8 @@ def permutation(layout: str, n: int, b: int = 16) -> np.ndarray:
         lib().orc_permute_btree(A, n, b)
     elif layout == "mveb":
         lib().orc_permute_mveb(A, n)
+    elif layout == "veb":
+        lib().orc_permute_veb_std(A, n)
     else:
         raise ValueError(layout)
     return A
@@ -89,8 +95,8 @@ def search(layout: str, A: np.ndarray, queries: np.ndarray, b: int = 16) -> np.n
         lib().orc_search_bst(A64, n, q64, len(q64), ans)
     elif layout == "btree":
         lib().orc_search_btree(A64, n, b, q64, len(q64), ans)
-    elif layout == "mveb":
-        tables, idx, table_idx, d = veb_tables(n)
+    elif layout in ("mveb", "veb"):
+        tables, idx, table_idx, d = veb_tables(n, standard=layout == "veb")
         if len(idx) == 1:
             lib().orc_search_veb(A64, tables.ctypes.data, n, d, q64, len(q64), ans)
         else:
@@ -115,22 +121,24 @@ def search_sorted(keys: np.ndarray, queries: np.ndarray) -> np.ndarray:
     return np.where(hit, lb, n).astype(np.uint64)
 
 
-def build_table(n: int, d: int) -> np.ndarray:
+def build_table(n: int, d: int, standard: bool = False) -> np.ndarray:
     t = np.zeros(max(d, 1), dtype=VEB_DTYPE)
-    lib().orc_build_table(t.ctypes.data, n, d, 0)
+    (lib().orc_build_table_std if standard else lib().orc_build_table)(t.ctypes.data, n, d, 0)
     return t
 
 
-def veb_tables(n: int):
-    """(tables, idx, table_idx, d) exactly as the reference's query driver builds
-    them (gpu/test/query-mveb-fixedN.cu:43-165); one table for perfect n."""
+def veb_tables(n: int, standard: bool = False):
+    """(tables, idx, table_idx, d) exactly as the reference's query drivers build
+    them: gpu/test/query-mveb-fixedN.cu:43-165 (mvEB), cpu/test/query-veb-fixedN.cpp:
+    37-150 (standard vEB); one table for perfect n."""
+    suf = "_std" if standard else ""
     nt = C.c_uint32()
     ts = C.c_uint32()
-    lib().orc_veb_tables_size(n, C.byref(nt), C.byref(ts))
+    getattr(lib(), f"orc_veb_tables_size{suf}")(n, C.byref(nt), C.byref(ts))
     tables = np.zeros(ts.value, dtype=VEB_DTYPE)
     idx = np.zeros(nt.value, dtype=np.uint64)
     table_idx = np.zeros(nt.value, dtype=np.uint32)
-    lib().orc_build_veb_tables(n, tables.ctypes.data, idx, table_idx)
+    getattr(lib(), f"orc_build_veb_tables{suf}")(n, tables.ctypes.data, idx, table_idx)
     return tables, idx, table_idx, int(n).bit_length()
 
 
@@ -154,6 +162,13 @@ def ref_cpu():
                                                C.c_uint64, C.c_uint32]
         L.ref_cpu_search_bst_u64.argtypes = [_u64p, C.c_uint64, _u64p, _u64p, C.c_uint64,
                                              C.c_uint32]
+        L.ref_cpu_permute_veb_u64.argtypes = [_u64p, C.c_uint64, C.c_uint32]
+        L.ref_cpu_permute_veb_u64.restype = C.c_double
+        L.ref_cpu_build_table.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32]
+        L.ref_cpu_search_veb_u64.argtypes = [_u64p, C.c_void_p, C.c_uint64, C.c_uint32, _u64p, _u64p,
+                                             C.c_uint64, C.c_uint32]
+        L.ref_cpu_search_veb_nonperfect_u64.argtypes = [_u64p, C.c_void_p, _u32p, _u64p, C.c_uint32,
+                                                        C.c_uint32, _u64p, _u64p, C.c_uint64, C.c_uint32]
         _ref_cpu = L
     return _ref_cpu
 

@@ -4,8 +4,10 @@
       B-tree / BST layouts and query answers from the reference's own CPU code
       (cpu/src/btree-cycles.h, cpu/src/bst-involutions.h, cpu/src/query-*.h) and
       mvEB position tables from the reference's buildTable
-      (gpu/src/query-mveb.cu, host code), both compiled from the reference
-      sources by oracle/Makefile into oracle/_ref/.
+      (gpu/src/query-mveb.cu, host code); standard vEB layouts, tables and
+      hit-only query answers from cpu/src/veb-cycles.h, cpu/src/query-veb.cpp
+      and cpu/src/query-veb.h; all compiled from the reference sources by
+      oracle/Makefile into oracle/_ref/.
   python tests/golden/make_golden.py gpu OUT.json
       mvEB layouts from the reference's own GPU permutation
       (gpu/src/mveb-cycles.cuh, timePermutevEB) run on a B200; needs
@@ -65,7 +67,8 @@ def make_cpu(out_path: str) -> None:
     ref = O.ref_cpu()
     assert ref is not None, "build oracle/_ref/libref_cpu.so first (make -C oracle)"
     out = {"source": "reference cpu/src compiled by oracle/Makefile", "btree": [], "bst": [],
-           "query_btree": [], "query_bst": [], "tables": [], "examples": []}
+           "query_btree": [], "query_bst": [], "tables": [], "examples": [],
+           "veb_std": [], "veb_std_tables": [], "query_veb_std": []}
     for b in BTREE_BS:
         for n in btree_sizes(b):
             A = np.arange(n, dtype=np.uint64)
@@ -110,6 +113,31 @@ def make_cpu(out_path: str) -> None:
         t = np.zeros(d, dtype=O.VEB_DTYPE)
         gpu.ref_gpu_build_table(t.ctypes.data, n, d, 0)
         out["tables"].append({"n": n, "d": d, "L": t["L"].tolist(), "R": t["R"].tolist(), "D": t["D"].tolist()})
+    # standard vEB (the reference's CPU layout): layouts, tables, hit-only answers
+    for n in MVEB_SIZES:
+        A = np.arange(n, dtype=np.uint64)
+        ref.ref_cpu_permute_veb_u64(A, n, 1)
+        out["veb_std"].append({"n": n, "sha": sha(A)})
+    for n in [3, 7, 15, 31, 63, 127, 255, 511, 1023, 2**16 - 1, 2**17 - 1, 2**20 - 1, 2**29 - 1, 2**30 - 1,
+              2**31 - 1, 2**33 - 1]:
+        d = n.bit_length()
+        t = np.zeros(d, dtype=O.VEB_DTYPE)
+        ref.ref_cpu_build_table(t.ctypes.data, n, d, 0)
+        out["veb_std_tables"].append({"n": n, "d": d, "L": t["L"].tolist(), "R": t["R"].tolist(),
+                                      "D": t["D"].tolist()})
+    for (n, q, seed) in [(2**20 - 1, 20000, 21), (100000, 5000, 22), (777, 3000, 23), (3000017, 20000, 24),
+                         (65536, 5000, 25)]:
+        keys = data.sorted_keys_np(n, 1, 16, seed)
+        Q = data.queries_np(keys, q, 1.0, seed + 1)  # hits only (see ref_cpu_search_veb_u64)
+        A = keys.copy()
+        ref.ref_cpu_permute_veb_u64(A, n, 1)
+        tables, idx, table_idx, d = O.veb_tables(n, standard=True)
+        ans = np.empty(q, dtype=np.uint64)
+        if len(idx) == 1:
+            ref.ref_cpu_search_veb_u64(A, tables.ctypes.data, n, d, Q, ans, q, 1)
+        else:
+            ref.ref_cpu_search_veb_nonperfect_u64(A, tables.ctypes.data, table_idx, idx, len(idx), d, Q, ans, q, 1)
+        out["query_veb_std"].append({"n": n, "q": q, "seed": seed, "sha": sha(ans), "hits": int((ans != n).sum())})
     with open(out_path, "w") as f:
         json.dump(out, f, separators=(",", ":"))
 

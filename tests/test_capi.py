@@ -39,7 +39,7 @@ SIZES = list(range(1, 130)) + [255, 256, 4095, 4096, 4097, 8191, 8193, 65535, 65
 
 
 @pytest.mark.parametrize("layout,b", [("bst", 1), ("btree", 2), ("btree", 3), ("btree", 8), ("btree", 16),
-                                      ("btree", 31), ("mveb", 0)])
+                                      ("btree", 31), ("mveb", 0), ("veb", 0)])
 def test_tile_schedule_replay_matches_oracle(layout, b):
     for n in SIZES:
         keys = np.arange(n, dtype=np.uint64) * 5 + 11

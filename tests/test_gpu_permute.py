@@ -21,7 +21,7 @@ SMALL = list(range(1, 301))
 EDGE = [511, 512, 1023, 1024, 4095, 4096, 4097, 8191, 8192, 8193, 16383, 16385, 65535, 65536, 65537,
         83520, 83521, 100003, 131071, 262143, 300001, 1048575, 1048576, 2097151, 3000017]
 CASES = [("bst", 1), ("btree", 2), ("btree", 3), ("btree", 8), ("btree", 16), ("btree", 17), ("btree", 32),
-         ("mveb", 0)]
+         ("mveb", 0), ("veb", 0)]
 
 
 def run(layout, keys, b, **kw):
@@ -46,7 +46,7 @@ def test_edge_sizes_bit_exact(layout, b, dtype):
         assert np.array_equal(run(layout, keys, b), O.permute(layout, keys, b or 16)), (layout, b, n)
 
 
-@pytest.mark.parametrize("layout,b", [("bst", 1), ("btree", 16), ("mveb", 0)])
+@pytest.mark.parametrize("layout,b", [("bst", 1), ("btree", 16), ("mveb", 0), ("veb", 0)])
 @pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
 def test_unaligned_base_pointer(layout, b, dtype):
     import torch
@@ -78,6 +78,8 @@ def test_caller_supplied_workspace_and_timing():
     ("mveb", 0, 2**24 - 1, np.uint32),
     ("mveb", 0, 30_000_001, np.uint32),
     ("btree", 8, 9_999_991, np.uint64),
+    ("veb", 0, 2**23 - 1, np.uint64),
+    ("veb", 0, 2**24 + 12_345, np.uint32),
 ])
 def test_medium_sizes_bit_exact(layout, b, n, dtype):
     keys = data.sorted_keys_np(n, 1, 3 if dtype == np.uint32 else 16, n % 1000, dtype)
@@ -115,6 +117,8 @@ def _full_size_properties(layout, b, n, key_bytes, gap):
     ("mveb", 0, 300_000_000, 4, 3),
     ("bst", 1, 2**28 - 1, 8, 16),
     ("btree", 16, 2**28, 8, 16),
+    ("veb", 0, 2**30 - 1, 4, 3),
+    ("veb", 0, 300_000_000, 4, 3),
 ])
 def test_full_size_properties(layout, b, n, kb, gap):
     _full_size_properties(layout, b, n, kb, gap)

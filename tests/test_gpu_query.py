@@ -28,7 +28,7 @@ def gpu_answers(layout, tree, Q, b=16):
 
 
 @pytest.mark.parametrize("layout,b", [("bst", 1), ("btree", 16), ("btree", 8), ("btree", 3), ("btree", 32),
-                                      ("btree", 1), ("btree", 64), ("mveb", 0)])
+                                      ("btree", 1), ("btree", 64), ("mveb", 0), ("veb", 0)])
 @pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
 def test_queries_match_oracle(layout, b, dtype):
     for n in [1, 2, 3, 5, 16, 17, 100, 255, 1000, 4097, 65535, 70001, 1048575, 3000017]:
@@ -64,6 +64,15 @@ def test_queries_match_reference_golden():
         keys = data.sorted_keys_np(e["n"], 1, 16, e["seed"])
         Q = data.queries_np(keys, e["q"], 0.5, e["seed"] + 1)
         assert sha(gpu_answers("bst", O.permute("bst", keys), Q)) == e["sha"]
+
+
+def test_standard_veb_queries_match_reference_golden():
+    with open(os.path.join(GOLD, "golden_cpu.json")) as f:
+        g = json.load(f)
+    for e in g["query_veb_std"]:
+        keys = data.sorted_keys_np(e["n"], 1, 16, e["seed"])
+        Q = data.queries_np(keys, e["q"], 1.0, e["seed"] + 1)
+        assert sha(gpu_answers("veb", O.permute("veb", keys), Q)) == e["sha"], e["n"]
 
 
 def test_benchmark_query_shapes_small():

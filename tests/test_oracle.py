@@ -2,8 +2,9 @@
 
 Golden fixtures in tests/golden/ were produced by the reference's own code
 compiled from its sources (tests/golden/make_golden.py): B-tree/BST layouts and
-query answers from cpu/src, mvEB tables from gpu/src/query-mveb.cu, and mvEB
-layouts from gpu/src/mveb-cycles.cuh run on a B200.
+query answers from cpu/src, mvEB tables from gpu/src/query-mveb.cu, mvEB
+layouts from gpu/src/mveb-cycles.cuh run on a B200, and the standard vEB
+layouts, tables and query answers of cpu/src/veb-cycles.h and query-veb.*.
 """
 import hashlib
 import json
@@ -66,6 +67,27 @@ def test_veb_tables_match_reference(gold):
     for e in gold["tables"]:
         t = O.build_table(e["n"], e["d"])
         assert t["L"].tolist() == e["L"] and t["R"].tolist() == e["R"] and t["D"].tolist() == e["D"], e["n"]
+
+
+def test_standard_veb_layouts_match_reference(gold):
+    bad = [e["n"] for e in gold["veb_std"] if sha(O.permutation("veb", e["n"])) != e["sha"]]
+    assert not bad, bad[:10]
+    assert len(gold["veb_std"]) > 300
+
+
+def test_standard_veb_tables_match_reference(gold):
+    for e in gold["veb_std_tables"]:
+        t = O.build_table(e["n"], e["d"], standard=True)
+        assert t["L"].tolist() == e["L"] and t["R"].tolist() == e["R"] and t["D"].tolist() == e["D"], e["n"]
+
+
+def test_standard_veb_queries_match_reference(gold):
+    for e in gold["query_veb_std"]:
+        keys = data.sorted_keys_np(e["n"], 1, 16, e["seed"])
+        Q = data.queries_np(keys, e["q"], 1.0, e["seed"] + 1)
+        ans = O.search("veb", O.permute("veb", keys), Q)
+        assert sha(ans) == e["sha"], e
+        assert int((ans != e["n"]).sum()) == e["hits"] == e["q"]
 
 
 def _mveb_pos_def(n, s):

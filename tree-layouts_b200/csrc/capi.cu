@@ -36,23 +36,25 @@ int sync_and_check(cudaStream_t st) {
     return TL_SUCCESS;
 }
 
-// buildTable: gpu/src/query-mveb.cu:25-47, with the mvEB split of
-// gpu/src/mveb-cycles.cuh:240-247.
-static void build_table(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
+// buildTable: gpu/src/query-mveb.cu:25-47 with the mvEB split of
+// gpu/src/mveb-cycles.cuh:240-247 (modified), cpu/src/query-veb.cpp:25-41 with
+// the standard split (the recursion is the same).
+static void build_table(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth, bool modified) {
     if (n == 1 || d < 2) return;
     uint32_t rd, ld;
-    mveb_split(d, rd, ld);
+    veb_split(d, modified, rd, ld);
     uint64_t root_n = low_mask(rd), leaf_n = low_mask(ld);
     uint32_t i = d - ld;
     table[i].L = leaf_n;
     table[i].R = root_n;
     table[i].D = root_depth;
-    build_table(table, root_n, rd, root_depth);
-    build_table(&table[i], leaf_n, ld, i + root_depth);
+    build_table(table, root_n, rd, root_depth, modified);
+    build_table(&table[i], leaf_n, ld, i + root_depth, modified);
 }
 
-// Table-set sizing: gpu/test/query-mveb-fixedN.cu:45-97.
-static void tables_size(uint64_t n, uint32_t &nt, uint32_t &ts, uint32_t &d) {
+// Table-set sizing: gpu/test/query-mveb-fixedN.cu:45-97 (modified),
+// cpu/test/query-veb-fixedN.cpp:37-84 (standard).
+static void tables_size(uint64_t n, uint32_t &nt, uint32_t &ts, uint32_t &d, bool modified) {
     d = bit_length(n);
     nt = 1;
     ts = d;
@@ -61,7 +63,7 @@ static void tables_size(uint64_t n, uint32_t &nt, uint32_t &ts, uint32_t &d) {
     uint32_t td = d;
     while (td >= 2) {
         uint32_t rd, ld;
-        mveb_split(td, rd, ld);
+        veb_split(td, modified, rd, ld);
         uint64_t r = low_mask(rd), l = low_mask(ld);
         uint64_t nf = (tn - r) / l, inc = tn - r - nf * l;
         if (inc == 0) break;
@@ -132,8 +134,8 @@ int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_
 
 int tl_layout_position(int layout, uint64_t n, uint64_t b, uint64_t rank, uint64_t *pos) {
     if (!pos || rank >= n) return TL_ERROR_INVALID_VALUE;
-    if (layout == TL_LAYOUT_MVEB) {
-        *pos = mveb_pos(n, rank);
+    if (is_veb_layout(layout)) {
+        *pos = veb_pos(n, rank, layout == TL_LAYOUT_MVEB);
         return TL_SUCCESS;
     }
     if (layout == TL_LAYOUT_BST) b = 1;
@@ -181,27 +183,45 @@ int tl_permute_mveb_u64(uint64_t *A, uint64_t n, void *s, float *ms) {
     return permute(TL_LAYOUT_MVEB, A, n, 0, 8, nullptr, 0, S(s), ms);
 }
 
-void tl_build_table(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
-    if (table) build_table(table, n, d, root_depth);
+int tl_permute_veb_std_u32(uint32_t *A, uint64_t n, void *s, float *ms) {
+    return permute(TL_LAYOUT_VEB, A, n, 0, 4, nullptr, 0, S(s), ms);
+}
+int tl_permute_veb_std_u64(uint64_t *A, uint64_t n, void *s, float *ms) {
+    return permute(TL_LAYOUT_VEB, A, n, 0, 8, nullptr, 0, S(s), ms);
 }
 
-int tl_veb_tables_size(uint64_t n, uint32_t *num_tables, uint32_t *table_size, uint32_t *d) {
+void tl_build_table(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
+    if (table) build_table(table, n, d, root_depth, true);
+}
+void tl_build_table_std(tl_veb_table *table, uint64_t n, uint32_t d, uint32_t root_depth) {
+    if (table) build_table(table, n, d, root_depth, false);
+}
+
+static int veb_tables_size(uint64_t n, uint32_t *num_tables, uint32_t *table_size, uint32_t *d, bool modified) {
     if (n == 0 || !num_tables || !table_size) return TL_ERROR_INVALID_VALUE;
     uint32_t nt, ts, dd;
-    tables_size(n, nt, ts, dd);
+    tables_size(n, nt, ts, dd, modified);
     *num_tables = nt;
     *table_size = ts;
     if (d) *d = dd;
     return TL_SUCCESS;
 }
+int tl_veb_tables_size(uint64_t n, uint32_t *num_tables, uint32_t *table_size, uint32_t *d) {
+    return veb_tables_size(n, num_tables, table_size, d, true);
+}
+int tl_veb_tables_size_std(uint64_t n, uint32_t *num_tables, uint32_t *table_size, uint32_t *d) {
+    return veb_tables_size(n, num_tables, table_size, d, false);
+}
 
-// Table-set construction: gpu/test/query-mveb-fixedN.cu:130-165.
-int tl_build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx) {
+// Table-set construction: gpu/test/query-mveb-fixedN.cu:130-165 (modified),
+// cpu/test/query-veb-fixedN.cpp:116-150 (standard; concatenated with table_idx
+// offsets as the GPU driver lays its tables out).
+static int build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx, bool modified) {
     if (n == 0 || !tables || !idx || !table_idx) return TL_ERROR_INVALID_VALUE;
     uint32_t nt, ts, d;
-    tables_size(n, nt, ts, d);
+    tables_size(n, nt, ts, d, modified);
     memset(tables, 0, ts * sizeof(tl_veb_table));
-    build_table(tables, n, d, 0);
+    build_table(tables, n, d, 0, modified);
     idx[nt - 1] = n;
     table_idx[0] = 0;
     uint64_t tn = n;
@@ -209,16 +229,22 @@ int tl_build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_
     for (uint32_t i = 1; i < nt; ++i) {
         table_idx[i] = table_idx[i - 1] + td;
         uint32_t rd, ld;
-        mveb_split(td, rd, ld);
+        veb_split(td, modified, rd, ld);
         uint64_t r = low_mask(rd), l = low_mask(ld);
         uint64_t nf = (tn - r) / l, inc = tn - r - nf * l;
         uint32_t id = bit_length(inc);
-        build_table(&tables[table_idx[i]], inc, id, 0);
+        build_table(&tables[table_idx[i]], inc, id, 0, modified);
         idx[i - 1] = n - inc;
         tn = inc;
         td = id;
     }
     return TL_SUCCESS;
+}
+int tl_build_veb_tables(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx) {
+    return build_veb_tables(n, tables, idx, table_idx, true);
+}
+int tl_build_veb_tables_std(uint64_t n, tl_veb_table *tables, uint64_t *idx, uint32_t *table_idx) {
+    return build_veb_tables(n, tables, idx, table_idx, false);
 }
 
 int tl_batch_plan_create(const int64_t *off, uint32_t num, uint64_t b, uint32_t kb, void *stream,

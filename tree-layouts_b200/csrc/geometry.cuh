@@ -15,7 +15,9 @@
 // = next power of two >= ceil(d/2) (:240-247).  Layout = [top | full bottoms |
 // incomplete bottom]; keys of the top that follow the incomplete bottom in sorted
 // order are the roots of the empty bottom slots (:344-380).  Every part is laid
-// out recursively with the same rule (:382-413).
+// out recursively with the same rule (:382-413).  The standard van Emde Boas
+// layout of the reference's CPU code (cpu/src/veb-cycles.h:33-173) is the same
+// recursion with leaf_d = ceil(d/2) unrounded.
 #pragma once
 
 #include "tl_common.cuh"
@@ -107,10 +109,14 @@ TL_HD uint64_t btree_top_rank(const BtreeGeom &g, uint64_t c) {
 }
 
 // ------------------------------------------------------------------ mvEB
-TL_HD void mveb_split(uint32_t d, uint32_t &root_d, uint32_t &leaf_d) {
+// Split of a tree of d levels into a top of root_d and bottoms of leaf_d levels:
+// root_d = floor((d - 2) / 2) + 1 (cpu/src/veb-cycles.h:118-119,
+// gpu/src/mveb-cycles.cuh:240-242), and for the modified layout leaf_d rounded
+// up to a power of two (gpu/src/mveb-cycles.cuh:243-246).
+TL_HD void veb_split(uint32_t d, bool modified, uint32_t &root_d, uint32_t &leaf_d) {
     root_d = (d - 2) / 2 + 1;
     leaf_d = d - root_d;
-    if (leaf_d & (leaf_d - 1)) {  // not a power of two: round up (mveb-cycles.cuh:243-246)
+    if (modified && (leaf_d & (leaf_d - 1))) {
         uint32_t p = 1;
         while (p < leaf_d) p <<= 1;
         leaf_d = p;
@@ -118,13 +124,15 @@ TL_HD void mveb_split(uint32_t d, uint32_t &root_d, uint32_t &leaf_d) {
     }
 }
 
-// Position of sorted rank s in the mvEB layout of n keys.
-TL_HD uint64_t mveb_pos(uint64_t n, uint64_t s) {
+TL_HD void mveb_split(uint32_t d, uint32_t &root_d, uint32_t &leaf_d) { veb_split(d, true, root_d, leaf_d); }
+
+// Position of sorted rank s in the (modified or standard) vEB layout of n keys.
+TL_HD uint64_t veb_pos(uint64_t n, uint64_t s, bool modified) {
     uint64_t pos = 0, nn = n;
     for (;;) {
         if (nn <= 1) return pos;
         uint32_t d = bit_length(nn), rd, ld;
-        mveb_split(d, rd, ld);
+        veb_split(d, modified, rd, ld);
         uint64_t r = low_mask(rd), l = low_mask(ld);
         uint64_t nf = (nn - r) / l, inc = nn - r - nf * l;
         uint64_t full = nf << ld;  // nf * (l + 1)
@@ -149,6 +157,8 @@ TL_HD uint64_t mveb_pos(uint64_t n, uint64_t s) {
     }
 }
 
+TL_HD uint64_t mveb_pos(uint64_t n, uint64_t s) { return veb_pos(n, s, true); }
+
 // A contiguous source range of the mvEB permutation.  Unit regions (U > 0) hold
 // the full bottom trees of one recursion segment: every aligned group of 2^U keys
 // is one "unit" (a bottom-level subtree of U levels, 2^U - 1 consecutive ranks
@@ -160,6 +170,7 @@ struct MvebRegion {
     uint64_t dst;         // destination of the segment's top tree
     uint64_t r, l;        // segment's top-tree and bottom-tree sizes
     uint32_t H, U;        // bottom-tree height, unit height (0: tail region)
+    uint32_t modified;    // split rule of the layout (1: mvEB, 0: standard vEB)
     uint64_t slot_base;   // first scratch slot of the region
     uint64_t tile_base;   // first tile of the region (tiles ascend with source position)
     uint64_t tile_len;    // keys per tile (a multiple of 2^U)
@@ -170,32 +181,49 @@ constexpr int kMaxRegions = 40;
 
 struct MvebPlan {
     uint64_t n = 0;
+    uint32_t modified = 1;  // 1: mvEB, 0: standard vEB
     int nreg = 0;
     MvebRegion reg[kMaxRegions];
     uint64_t total_slots = 0, total_tiles = 0;
 };
 
 // Destination of the first key of unit g (0-based, counted from the start of the
-// region) for bottoms of H levels split down to units of U levels.
+// region) for bottoms of H levels split down to units of U levels: at each split
+// of h levels into a top of rt and bottoms of lf levels, every bottom holds
+// 2^(lf - U) units, so the unit index picks a bottom with its high bits.
 TL_HD uint64_t mveb_unit_dst(const MvebRegion &R, uint64_t g) {
     uint32_t per_bottom_bits = R.H - R.U;
     uint64_t off = R.dst + R.r + (g >> per_bottom_bits) * R.l;
     uint64_t j = g & low_mask(per_bottom_bits);
     uint32_t h = R.H;
     while (h > R.U) {
-        uint32_t half = h >> 1;
-        uint64_t sub = low_mask(half);  // size of the top and of each bottom at this split
-        uint32_t jb = half - R.U;
-        off += sub + (j >> jb) * sub;
+        uint32_t rt, lf;
+        veb_split(h, R.modified != 0, rt, lf);
+        const uint32_t jb = lf - R.U;
+        off += low_mask(rt) + (j >> jb) * low_mask(lf);
         j &= low_mask(jb);
-        h = half;
+        h = lf;
     }
     return off;
 }
 
-__host__ inline MvebPlan make_mveb_plan(uint64_t n, uint32_t unit_max_levels, uint64_t tile_keys) {
+// Height of the units of a bottom of H levels: follow the bottoms of its
+// recursion until they have at most unit_max levels.
+TL_HD uint32_t veb_unit_levels(uint32_t H, bool modified, uint32_t unit_max) {
+    uint32_t h = H;
+    while (h > unit_max) {
+        uint32_t rt, lf;
+        veb_split(h, modified, rt, lf);
+        h = lf;
+    }
+    return h;
+}
+
+__host__ inline MvebPlan make_mveb_plan(uint64_t n, uint32_t unit_max_levels, uint64_t tile_keys,
+                                       bool modified = true) {
     MvebPlan P;
     P.n = n;
+    P.modified = modified ? 1 : 0;
     MvebRegion tails[kMaxRegions];
     int ntails = 0;
     uint64_t src = 0, dst = 0, nn = n;
@@ -208,7 +236,7 @@ __host__ inline MvebPlan make_mveb_plan(uint64_t n, uint32_t unit_max_levels, ui
             break;
         }
         uint32_t d = bit_length(nn), rd, ld;
-        mveb_split(d, rd, ld);
+        veb_split(d, modified, rd, ld);
         uint64_t r = low_mask(rd), l = low_mask(ld);
         uint64_t nf = (nn - r) / l, inc = nn - r - nf * l;
         uint64_t full = nf << ld;
@@ -219,7 +247,8 @@ __host__ inline MvebPlan make_mveb_plan(uint64_t n, uint32_t unit_max_levels, ui
         u.r = r;
         u.l = l;
         u.H = ld;
-        u.U = ld < unit_max_levels ? ld : unit_max_levels;
+        u.U = veb_unit_levels(ld, modified, unit_max_levels);
+        u.modified = P.modified;
         P.reg[P.nreg++] = u;
         uint64_t after = src + full + inc;
         if (full < nn && after < src + nn) {  // roots of the empty bottom slots

@@ -10,6 +10,9 @@ namespace tl {
 
 void record_cuda_error(cudaError_t e);
 
+// The two van Emde Boas layouts share one permutation engine (split rule aside).
+inline bool is_veb_layout(int layout) { return layout == TL_LAYOUT_MVEB || layout == TL_LAYOUT_VEB; }
+
 #define TL_CUDA_TRY(expr)                       \
     do {                                        \
         cudaError_t tl_e_ = (expr);             \

@@ -101,10 +101,14 @@ static int make_bulk_plan(const BtreeStream &S, const K *A, const K *scr, BulkPl
 }
 
 // ---------------------------------------------------------------- mvEB stream
+// Unit tables: for a unit of U levels (1 <= U <= 8), inv[unit_table_off(U) + q]
+// is the sorted rank (within the unit) held at unit position q.
+TL_HD uint32_t unit_table_off(uint32_t U) { return (1u << U) - U - 1; }  // sum of 2^u - 1 over u < U
+constexpr uint32_t kUnitTableBytes = (1u << 9) - 9 - 1;                   // unit_table_off(9)
+
 struct MvebParams {
     MvebPlan plan;
-    // inv_perm_U[q]: sorted rank (within a unit of U levels) at unit position q.
-    unsigned char inv1[1], inv2[3], inv4[15], inv8[255];
+    unsigned char inv[kUnitTableBytes];
 };
 
 TL_HD int mveb_region_of_tile(const MvebPlan &P, uint64_t k) {
@@ -181,7 +185,7 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
         mveb_tile(P, k, ri, p0, p1);
         const MvebRegion &R = P.reg[ri];
         if ((int)R.U != loaded_U && R.U) {  // block-uniform: unit tables for this height
-            const unsigned char *src = R.U == 8 ? prm.inv8 : R.U == 4 ? prm.inv4 : R.U == 2 ? prm.inv2 : prm.inv1;
+            const unsigned char *src = prm.inv + unit_table_off(R.U);
             for (uint32_t q = threadIdx.x; q < (1u << R.U) - 1; q += blockDim.x) s_inv[q] = src[q];
             loaded_U = R.U;
         }
@@ -228,25 +232,23 @@ mveb_scatter_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_c
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const uint64_t rank = mveb_slot_rank(P, s + u * stride);
-            if (rank != ~0ull) A[mveb_pos(P.n, rank)] = v[u];
+            if (rank != ~0ull) A[veb_pos(P.n, rank, P.modified != 0)] = v[u];
         }
     }
     for (; s < P.total_slots; s += stride) {
         const uint64_t rank = mveb_slot_rank(P, s);
-        if (rank != ~0ull) A[mveb_pos(P.n, rank)] = scr[s];
+        if (rank != ~0ull) A[veb_pos(P.n, rank, P.modified != 0)] = scr[s];
     }
 }
 
 // ---------------------------------------------------------------- host side
 static void fill_unit_tables(MvebParams &prm) {
-    auto fill = [](unsigned char *inv, uint32_t U) {
-        uint64_t m = (1ull << U) - 1;
-        for (uint64_t s = 0; s < m; ++s) inv[mveb_pos(m, s)] = (unsigned char)s;
-    };
-    fill(prm.inv1, 1);
-    fill(prm.inv2, 2);
-    fill(prm.inv4, 4);
-    fill(prm.inv8, 8);
+    const bool modified = prm.plan.modified != 0;
+    for (uint32_t U = 1; U <= 8; ++U) {
+        unsigned char *inv = prm.inv + unit_table_off(U);
+        const uint64_t m = (1ull << U) - 1;
+        for (uint64_t s = 0; s < m; ++s) inv[veb_pos(m, s, modified)] = (unsigned char)s;
+    }
 }
 
 struct PermutePlan {
@@ -263,15 +265,15 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
     if (key_bytes != 4 && key_bytes != 8) return TL_ERROR_INVALID_VALUE;
     if (layout == TL_LAYOUT_BST) b = 1;
     if (layout == TL_LAYOUT_BTREE && b == 0) return TL_ERROR_INVALID_VALUE;
-    if (layout < TL_LAYOUT_BST || layout > TL_LAYOUT_MVEB) return TL_ERROR_INVALID_VALUE;
+    if (layout < TL_LAYOUT_BST || layout > TL_LAYOUT_VEB) return TL_ERROR_INVALID_VALUE;
     pl.layout = layout;
     pl.key_bytes = key_bytes;
     pl.n = n;
     pl.b = b;
     pl.tile_keys = 32768 / key_bytes;
-    if (layout == TL_LAYOUT_MVEB) {
+    if (is_veb_layout(layout)) {
         if (n >= (1ull << 62)) return TL_ERROR_UNSUPPORTED;
-        pl.mp.plan = make_mveb_plan(n, kUnitMaxLevels, pl.tile_keys);
+        pl.mp.plan = make_mveb_plan(n, kUnitMaxLevels, pl.tile_keys, layout == TL_LAYOUT_MVEB);
         fill_unit_tables(pl.mp);
         pl.ntiles = pl.mp.plan.total_tiles;
         pl.scratch_keys = pl.mp.plan.total_slots;
@@ -324,7 +326,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
     TL_CUDA_TRY(cudaMemsetAsync(flags, 0, pl.bytes - pl.off_flags, st));
     const size_t smem = (size_t)pl.tile_keys * sizeof(K) + 16;  // the tile plus its 16-byte head slack
     const int smx = sm_count();
-    if (pl.layout == TL_LAYOUT_MVEB) {
+    if (is_veb_layout(pl.layout)) {
         auto kern = mveb_stream_kernel<K>;
         TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
@@ -396,7 +398,7 @@ int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes,
     PermutePlan pl;
     int rc = make_plan(layout, n, b, key_bytes, pl);
     if (rc) return rc;
-    if (layout == TL_LAYOUT_MVEB) {
+    if (is_veb_layout(layout)) {
         *keys = pl.mp.plan.total_slots;
     } else {
         *keys = 0;
@@ -473,7 +475,7 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
         std::vector<uint64_t> scr(pl.scratch_keys, 0), tile(pl.tile_keys + 1);
         std::vector<uint8_t> readk(pl.ntiles, 0), written(n, 0);
         std::vector<uint32_t> slot_writes(pl.scratch_keys, 0), pos_writes(n, 0);
-        const bool mv = pl.layout == TL_LAYOUT_MVEB;
+        const bool mv = is_veb_layout(pl.layout);
         const MvebPlan &P = pl.mp.plan;
         auto tile_of = [&](uint64_t d) { return mv ? mveb_tile_of(P, d) : d / pl.tile_keys; };
         for (uint64_t t = 0; t < pl.ntiles; ++t) {
@@ -587,8 +589,7 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                 if (R.U == 0) {
                     for (uint64_t x = p0; x < p1; ++x) SC(R.slot_base + (x - R.src), tile[x - p0]);
                 } else {
-                    const unsigned char *inv = R.U == 8 ? pl.mp.inv8 : R.U == 4 ? pl.mp.inv4
-                                             : R.U == 2 ? pl.mp.inv2 : pl.mp.inv1;
+                    const unsigned char *inv = pl.mp.inv + unit_table_off(R.U);
                     const uint64_t u = (1ull << R.U) - 1;
                     uint64_t g0, g1;
                     mveb_tile_groups(R, p0, p1, g0, g1);
@@ -622,7 +623,7 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                 const uint64_t rank = mveb_slot_rank(P, s2);
                 if (rank == ~0ull) { if (slot_writes[s2]) ++viol; continue; }
                 if (slot_writes[s2] != 1) ++viol;
-                const uint64_t d = mveb_pos(n, rank);
+                const uint64_t d = veb_pos(n, rank, P.modified != 0);
                 A[d] = scr[s2];
                 ++pos_writes[d];
             }

@@ -16,8 +16,9 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "libtreelayouts.so")
 
-LAYOUT_BST, LAYOUT_BTREE, LAYOUT_MVEB = 0, 1, 2
-LAYOUTS = {"bst": LAYOUT_BST, "btree": LAYOUT_BTREE, "mveb": LAYOUT_MVEB}
+LAYOUT_BST, LAYOUT_BTREE, LAYOUT_MVEB, LAYOUT_VEB = 0, 1, 2, 3
+# "veb": the standard van Emde Boas layout of the reference's CPU code
+LAYOUTS = {"bst": LAYOUT_BST, "btree": LAYOUT_BTREE, "mveb": LAYOUT_MVEB, "veb": LAYOUT_VEB}
 
 SUCCESS = 0
 ERROR_INVALID_VALUE = 1
@@ -64,8 +65,10 @@ def lib():
         L.tl_debug_set_wait.argtypes = [C.c_uint, C.c_int]
         L.tl_build_table.argtypes = [_v, _u64, _u32, _u32]
         L.tl_build_table.restype = None
-        L.tl_veb_tables_size.argtypes = [_u64, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32)]
-        L.tl_build_veb_tables.argtypes = [_u64, _v, _v, _v]
+        for suf in ("", "_std"):
+            getattr(L, f"tl_veb_tables_size{suf}").argtypes = [_u64, C.POINTER(_u32), C.POINTER(_u32),
+                                                               C.POINTER(_u32)]
+            getattr(L, f"tl_build_veb_tables{suf}").argtypes = [_u64, _v, _v, _v]
         for w in ("u32", "u64"):
             getattr(L, f"tl_query_bst_{w}").argtypes = [_v, _u64, _v, _u64, _v, _v, _f32p]
             getattr(L, f"tl_query_sorted_{w}").argtypes = [_v, _u64, _v, _u64, _v, _v, _f32p]
@@ -132,15 +135,18 @@ def build_table(n: int, d: int) -> np.ndarray:
     return t
 
 
-def veb_tables(n: int):
-    """(tables, idx, table_idx, d): the table set of a layout of n keys."""
+def veb_tables(n: int, standard: bool = False):
+    """(tables, idx, table_idx, d): the table set of an mvEB layout of n keys
+    (standard=True: of a standard vEB layout)."""
+    suf = "_std" if standard else ""
     nt, ts, d = _u32(), _u32(), _u32()
-    _check(lib().tl_veb_tables_size(n, C.byref(nt), C.byref(ts), C.byref(d)), "tl_veb_tables_size")
+    _check(getattr(lib(), f"tl_veb_tables_size{suf}")(n, C.byref(nt), C.byref(ts), C.byref(d)),
+           "tl_veb_tables_size")
     tables = np.zeros(ts.value, dtype=VEB_DTYPE)
     idx = np.zeros(nt.value, dtype=np.uint64)
     tidx = np.zeros(nt.value, dtype=np.uint32)
-    _check(lib().tl_build_veb_tables(n, tables.ctypes.data, idx.ctypes.data, tidx.ctypes.data),
-           "tl_build_veb_tables")
+    _check(getattr(lib(), f"tl_build_veb_tables{suf}")(n, tables.ctypes.data, idx.ctypes.data,
+                                                        tidx.ctypes.data), "tl_build_veb_tables")
     return tables, idx, tidx, d.value
 
 
@@ -163,11 +169,12 @@ def permute(layout: str, keys, b: int = 16, stream=None, workspace=None, timed: 
 
 
 class VebTablesDevice:
-    """Device copies of the mvEB table set for a layout of n keys."""
+    """Device copies of the table set for an mvEB (or, standard=True, a standard
+    vEB) layout of n keys."""
 
-    def __init__(self, n: int, device="cuda"):
+    def __init__(self, n: int, device="cuda", standard: bool = False):
         import torch
-        tables, idx, tidx, d = veb_tables(n)
+        tables, idx, tidx, d = veb_tables(n, standard)
         self.n, self.d, self.num_tables = n, d, len(idx)
         self.tables = torch.from_numpy(tables.view(np.uint8).copy()).to(device)
         self.idx = torch.from_numpy(idx.view(np.int64).copy()).to(device)
@@ -191,9 +198,9 @@ def query(layout: str, tree, queries, answers, b: int = 16, tables: VebTablesDev
     elif layout == "btree":
         rc = getattr(L, f"tl_query_btree_{w}")(tree.data_ptr(), n, b, queries.data_ptr(), q, answers.data_ptr(),
                                                s, msp)
-    elif layout == "mveb":
+    elif layout in ("mveb", "veb"):
         if tables is None:
-            tables = VebTablesDevice(n, tree.device)
+            tables = VebTablesDevice(n, tree.device, standard=layout == "veb")
         if tables.num_tables == 1:
             rc = getattr(L, f"tl_query_veb_{w}")(tree.data_ptr(), tables.tables.data_ptr(), n, tables.d,
                                                  queries.data_ptr(), q, answers.data_ptr(), s, msp)
