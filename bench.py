@@ -354,6 +354,7 @@ def run_ours(args, rank, world, local):
     if args.n:
         n = args.n
     L = T.lib()
+    L.tl_debug_set_schedule(1 if args.schedule == "fixed" else 0)
     L.tl_debug_permute_phases.argtypes = [C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p,
                                           C.POINTER(C.c_float)]
     dev = torch.device("cuda", local)
@@ -404,6 +405,11 @@ def run_ours(args, rank, world, local):
     if L.tl_debug_permute_scratch_keys(lay, n, b or 16, kb, C.byref(skeys)):
         raise RuntimeError("tl_debug_permute_scratch_keys")
     pass2_bytes = 2.0 * skeys.value * kb
+    stalls, polls = C.c_uint64(0), C.c_uint64(0)  # of the last timed permutation
+    L.tl_debug_wait_stats(C.byref(stalls), C.byref(polls))
+    L.tl_debug_permute_plan.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint32]
+    plan = L.tl_debug_permute_plan(lay, n, b or 16, kb)
+    pass2_kernel = {0: "btree_copy_kernel", 1: "btree_copy_kernel", 2: "btree_fix_kernel"}.get(plan, "mveb_scatter_kernel")
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"stream_traffic_{args.workload}.json")
     if os.path.exists(prof):
@@ -486,11 +492,14 @@ def run_ours(args, rank, world, local):
                        "restore": "array re-initialised from a pristine copy between steps, untimed",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": "mveb_stream_kernel" if layout in ("mveb", "veb") else "btree_stream_kernel",
+                         "schedule": {0: "right-to-left", 1: "left-to-right", 2: "ordered tiles"}.get(plan, "vEB units"),
+                         "stalled_waits": stalls.value, "stall_polls": polls.value,
+                         "blocks_per_sm": L.tl_debug_stream_blocks_per_sm(lay, kb),
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": f"hbm_gbs of {peak_kind}",
                          "traffic": traffic, "algorithmic_bytes_per_launch": int(bytes_step),
                          "stream_ms": round(stream_ms, 4),
-                         "pass2_kernel": "mveb_scatter_kernel" if layout in ("mveb", "veb") else "btree_copy_kernel",
+                         "pass2_kernel": pass2_kernel,
                          "pass2_ms": round(pass2_ms, 4), "pass2_bytes_per_launch": int(pass2_bytes),
                          "pass2_achieved": round(pass2_bytes / (pass2_ms * 1e-3) / 1e9, 1) if pass2_ms > 0 else None,
                          "whole_permute_frac": round(bytes_step / (ms_local * 1e-3) / 1e9 / peak, 4)},
@@ -524,6 +533,8 @@ def main():
     ap.add_argument("--batched", type=int, default=1, help="batched permute/query section (B-tree workloads)")
     ap.add_argument("--batch-num", type=int, default=4096)
     ap.add_argument("--batch-q", type=int, default=2**26)
+    ap.add_argument("--schedule", default="auto", choices=["auto", "fixed"],
+                    help="B-tree/BST stream schedule: the library's choice, or the fixed-direction ones only")
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

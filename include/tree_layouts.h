@@ -301,14 +301,28 @@ int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_
 /* sizeof of the ABI structs, for bindings to check their mirrors:
  * 0 tl_veb_table, 1 tl_rank_model, 2 tl_rank_leaf, 3 tl_rank_train_config. */
 int tl_debug_struct_size(int which);
-/* Schedule the B-tree permutation uses for (n, b): 0 right-to-left, 1 left-to-right. */
+/* Fixed-direction schedule of the B-tree permutation for (n, b): 0
+ * right-to-left, 1 left-to-right (the one tl_permute_static_ws takes). */
 int tl_debug_btree_plan(uint64_t n, uint64_t b);
+/* Schedule tl_permute takes for (layout, n, b, key_bytes) with a workspace of
+ * tl_permute_workspace_bytes: 0 right-to-left, 1 left-to-right, 2 ordered
+ * tiles (B-tree and BST from 64 tiles up), 3 the vEB engine; < 0 on error. */
+int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes);
+/* Resident blocks per SM of the stream kernel of `layout` at key_bytes (occupancy check). */
+int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes);
+/* fixed_only != 0: B-tree and BST permutations keep to the fixed-direction
+ * schedules (0 and 1 of tl_debug_permute_plan); 0 restores the default. */
+int tl_debug_set_schedule(int fixed_only);
+/* Of the last permutation's bounded waits: how many found their flag unset at
+ * the first look, and how many polls those took in total. */
+int tl_debug_wait_stats(uint64_t *stalled_waits, uint64_t *polls);
 /* Keys the permutation of (layout, n, b, key_bytes) moves through its scratch
  * buffer (the second pass reads and writes each once). */
 int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
 /* tl_permute with library-allocated workspace, reporting the device time of its
  * two passes: phase_ms[0] = setup + stream kernel, phase_ms[1] = the second pass
- * (B-tree: scratch copy kernel; mvEB: scratch scatter kernel). */
+ * (B-tree: scratch copy kernel, or the fix kernel of the ordered schedule;
+ * mvEB: scratch scatter kernel). */
 int tl_debug_permute_phases(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                             void *stream, float *phase_ms);
 

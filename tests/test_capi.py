@@ -98,3 +98,17 @@ def test_workspace_is_small_relative_to_input():
     # mvEB: about one key in 256 goes through scratch
     assert T.workspace_bytes("mveb", 2**30 - 1, 0, 4) < 4 * 2**30 // 100
     assert T.workspace_bytes("btree", n, 16, 8) > 0
+
+
+@pytest.mark.parametrize("layout,n,b", [("bst", 2**23 - 1, 1), ("btree", 29_000_000, 16), ("btree", 6_000_000, 8)])
+def test_ordered_schedule_replay_at_scale(layout, n, b):
+    """The ordered-tile schedule over thousands of tiles (the headline's shape at
+    1/17 of its size): chains, scratch tiles and the fix pass replayed with the
+    protocol checks, against the oracle."""
+    lib = T.lib()
+    lib.tl_debug_permute_plan.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint32]
+    assert lib.tl_debug_permute_plan(T.LAYOUTS[layout], n, b, 8) == 2
+    keys = np.arange(n, dtype=np.uint64) * 3 + 7
+    got, viol = T.emulate_permute(layout, keys, b)
+    assert viol == 0
+    assert np.array_equal(got, O.permute(layout, keys, b))

@@ -1,0 +1,209 @@
+// Plan O's tile order for the B-tree / BST stream pass, and its per-geometry cache.
+//
+// The stream pass stores a key straight into its final position only when the
+// tile under that position was read before the key's own tile; every other key
+// takes a second trip through scratch.  With tiles in position order (plans R
+// and L) the keys of whole levels go the wrong way: for a BST about 39 % of all
+// keys, for a B-tree with b = 16 and n = 2^30 about 38 %.  Here each tile u
+// names the tile that feeds it the most keys (pred(u), when that run holds at
+// least tile_keys / 8 of them) and gets the depth m(u) = 1 + m(pred(u)) of that
+// chain (0 without a pred, kChainCap on a cycle).  Tiles go in decreasing m, so
+// the heaviest edge into every tile points forward in the order and the chains
+// of leaf edges (and of the top tree's heavy levels) stay consistent; ties go
+// right to left or left to right, whichever leaves fewer scratch keys.  For
+// 8-byte keys this leaves 6.1 % of the keys of a b = 16 B-tree of 5e8 keys, 6.5 %
+// at 2^30 keys, 10 % of a b = 8 tree of 6e7 keys and 20 % of a BST of 2^30 - 1
+// keys for the second pass.
+//
+// The tables depend on (n, b, tile_keys) only.  They are computed once on the
+// host (O(tiles): a few source runs per tile) and copied once to each device
+// that uses them; both copies live until the process exits.  A geometry seen
+// for the first time while its stream is being captured gets no device copy
+// (the permutation then takes plan R or L).
+#include <algorithm>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "btree_order.h"
+#include "internal.h"
+
+namespace tl {
+
+constexpr uint32_t kChainCap = 64;
+constexpr size_t kMaxOrderEntries = 64;
+constexpr int kMaxOrderDevices = 64;
+
+// pred(u) for every tile: the source tile with the longest run into u.
+static void order_preds(const BtreeStream &S, std::vector<int64_t> &pred) {
+    const uint64_t N = S.ntiles, T = S.tile_keys, thr = T / 8;
+    pred.assign(N, -1);
+    for (uint64_t u = 0; u < N; ++u) {
+        const uint64_t P0 = u << S.tile_shift, P1 = std::min(P0 + T, S.g.n);
+        uint64_t best = 0;
+        int64_t bz = -1;
+        for (uint64_t a = P0; a < P1;) {
+            uint32_t lv;
+            uint64_t e;
+            btree_fix_piece(S, a, P1, lv, e);
+            if (e - a >= thr) {
+                const uint64_t z0 = btree_src_rank(S, a) >> S.tile_shift;
+                const uint64_t z1 = btree_src_rank(S, e - 1) >> S.tile_shift;
+                if (z1 - z0 <= 64)  // more runs than that are all shorter than thr
+                    for (uint64_t z = z0; z <= z1; ++z) {
+                        if (z == u) continue;
+                        uint64_t pa, pe;
+                        btree_fix_run(S, lv, a, e, z0, z1, z, pa, pe);
+                        if (pe - pa > best) {
+                            best = pe - pa;
+                            bz = (int64_t)z;
+                        }
+                    }
+            }
+            a = e;
+        }
+        if (best >= thr) pred[u] = bz;
+    }
+}
+
+// Tickets by decreasing chain depth m (counting sort), ties in position order
+// (asc) or against it; then the tiles that receive scratch keys, each given a
+// tile of scratch.  Returns the number of scratch keys.
+static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, bool asc, OrderVectors &v) {
+    const uint64_t N = S.ntiles;
+    std::vector<uint64_t> start(kChainCap + 1, 0);
+    for (uint64_t u = 0; u < N; ++u) ++start[m[u]];
+    uint64_t acc = 0;
+    for (int mm = (int)kChainCap; mm >= 0; --mm) {
+        const uint64_t c = start[mm];
+        start[mm] = acc;
+        acc += c;
+    }
+    v.tab.assign(N, make_uint2(0, kNoSlot));
+    v.order.assign(N, 0);
+    for (uint64_t i = 0; i < N; ++i) {
+        const uint64_t u = asc ? i : N - 1 - i;
+        const uint64_t t = start[m[u]]++;
+        v.order[t] = (uint32_t)u;
+        v.tab[u].x = (uint32_t)t;
+    }
+    S.tab = v.tab.data();
+    v.list.clear();
+    uint64_t keys = 0;
+    for (uint64_t u = 0; u < N; ++u) {
+        uint64_t c = 0;
+        btree_fix_tile_host(S, u, [&](uint64_t, uint64_t len) {
+            c += len;
+            return true;
+        });
+        if (!c) continue;
+        keys += c;
+        v.tab[u].y = (uint32_t)v.list.size();
+        v.list.push_back((uint32_t)u);
+    }
+    return keys;
+}
+
+void btree_compute_order(const BtreeStream &S0, OrderVectors &v) {
+    BtreeStream S = S0;
+    S.plan = PLAN_O;
+    const uint64_t N = S.ntiles;
+    std::vector<int64_t> pred;
+    order_preds(S, pred);
+    // chain depths, each path walked once (state 1: on the current path)
+    std::vector<uint8_t> m(N, 0), state(N, 0);
+    std::vector<uint64_t> path;
+    for (uint64_t u = 0; u < N; ++u) {
+        if (state[u] == 2) continue;
+        path.clear();
+        int64_t w = (int64_t)u;
+        while (w >= 0 && state[w] == 0) {
+            state[w] = 1;
+            path.push_back((uint64_t)w);
+            w = pred[w];
+        }
+        uint32_t cur = w < 0 ? 0 : state[w] == 1 ? kChainCap : std::min<uint32_t>(kChainCap, 1u + m[w]);
+        for (size_t j = path.size(); j-- > 0;) {
+            m[path[j]] = (uint8_t)cur;
+            state[path[j]] = 2;
+            cur = std::min<uint32_t>(kChainCap, cur + 1);
+        }
+    }
+    // both tie orders (right to left, left to right); keep the one with fewer scratch keys
+    OrderVectors w;
+    uint64_t best = UINT64_MAX;
+    for (int asc = 0; asc < 2; ++asc) {
+        const uint64_t c = order_by_depth(S, m, asc != 0, w);
+        if (c < best) {
+            best = c;
+            std::swap(v, w);
+        }
+    }
+}
+
+namespace {
+struct OrderEntry {
+    uint64_t n, b, tile_keys;
+    OrderVectors v;
+    void *dev[kMaxOrderDevices] = {};  // tab, then order and list
+};
+std::mutex g_order_mu;
+std::vector<std::unique_ptr<OrderEntry>> g_orders;
+
+OrderEntry *order_entry_locked(const BtreeStream &S) {
+    for (auto &e : g_orders)
+        if (e->n == S.g.n && e->b == S.g.b && e->tile_keys == S.tile_keys) return e.get();
+    if (g_orders.size() >= kMaxOrderEntries) return nullptr;
+    auto e = std::make_unique<OrderEntry>();
+    e->n = S.g.n;
+    e->b = S.g.b;
+    e->tile_keys = S.tile_keys;
+    btree_compute_order(S, e->v);
+    g_orders.push_back(std::move(e));
+    return g_orders.back().get();
+}
+}  // namespace
+
+bool btree_order_host(const BtreeStream &S, OrderTables &t) {
+    std::lock_guard<std::mutex> lk(g_order_mu);
+    OrderEntry *e = order_entry_locked(S);
+    if (!e) return false;
+    t = e->v.tables();
+    return true;
+}
+
+bool btree_order_device(const BtreeStream &S, cudaStream_t st, OrderTables &t) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxOrderDevices) return false;
+    std::lock_guard<std::mutex> lk(g_order_mu);
+    OrderEntry *e = order_entry_locked(S);
+    if (!e) return false;
+    const uint64_t N = S.ntiles, L = e->v.list.size();
+    if (!e->dev[dev]) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+        char *p = nullptr;
+        const size_t o1 = N * sizeof(uint2), o2 = o1 + N * sizeof(uint32_t);
+        if (cudaMalloc(reinterpret_cast<void **>(&p), o2 + L * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        // synchronous copies from pageable memory: done before the tables are used
+        if (cudaMemcpy(p, e->v.tab.data(), o1, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(p + o1, e->v.order.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+            (L && cudaMemcpy(p + o2, e->v.list.data(), L * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)) {
+            cudaGetLastError();
+            cudaFree(p);
+            return false;
+        }
+        e->dev[dev] = p;
+    }
+    const char *p = static_cast<const char *>(e->dev[dev]);
+    t.tab = reinterpret_cast<const uint2 *>(p);
+    t.order = reinterpret_cast<const uint32_t *>(p + N * sizeof(uint2));
+    t.list = t.order + N;
+    t.nlist = L;
+    return true;
+}
+
+}  // namespace tl

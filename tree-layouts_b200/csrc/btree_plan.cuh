@@ -32,11 +32,24 @@ constexpr int kMaxTopRuns = 2 * kMaxTopLevels;  // a tile holds at most two grou
 // plus the last level under plan L) into place, and the stream pass writes each
 // tile's top keys as contiguous runs, one per level.  seg1 is rounded so that
 // the copies see the same 16-byte alignment on both sides.
-enum BtreePlan { PLAN_R = 0, PLAN_L = 1 };
+//
+// Plan O (ordered) processes the tiles in a host-chosen order, rank[tile] being
+// a tile's ticket.  A key of source tile z goes straight to its final position
+// p when the tile u under p is z itself or was read before z (rank[u] <
+// rank[z]); otherwise it goes to scratch slot p + soff(u).  Only the tiles
+// that can receive such keys own scratch (a tile's worth each, in the order of
+// the host's list of them), so soff(u) = (slot[u] - u) * tile_keys with slot[u]
+// u's index in that list.  rank and slot share one 8-byte entry per tile
+// (tab[u]), so a tile's decision and its scratch offset are one load.  The order puts each tile before the tile that feeds it most keys,
+// following those edges in chains, so that far fewer keys go through scratch
+// than under either fixed direction.  Its second pass (btree_fix_tile_warp)
+// walks the listed tiles.
+enum BtreePlan { PLAN_R = 0, PLAN_L = 1, PLAN_O = 2 };
 
 struct BtreeStream {
     BtreeGeom g;
     FastDiv64 fd;         // b + 1
+    FastDiv64 fdb;        // b (b >= 2)
     FastDiv32 fd32;       // b + 1, for tile-local offsets
     FastDiv32 fd32b;      // b (unused when b = 1)
     uint64_t tile_keys, ntiles;
@@ -46,9 +59,52 @@ struct BtreeStream {
     uint64_t E;           // top-tree scratch slots: [0, E)
     uint64_t seg1;        // plan L: scratch slot of final position ni
     uint64_t nscratch;    // scratch slots
+    const uint2 *tab = nullptr;       // plan O: per tile {rank: its ticket, slot: its scratch tile or kNoSlot}
+    const uint32_t *order = nullptr;  // plan O: tile of each ticket
     uint64_t bnd[kMaxTopLevels];  // direct-store boundary position of level k
     FastDiv64 pdiv[kMaxTopLevels + 1];  // division by (b+1)^k, k >= 1 (host-built)
 };
+
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;  // tab[u].y of a tile that owns no scratch
+
+// Read-only table loads (the plan-O tables do not change during a launch).
+TL_HD uint32_t ld_table(const uint32_t *p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+TL_HD uint2 ld_entry(const uint2 *p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
+// Records an inconsistent schedule (a scratch store into a tile without scratch).
+__device__ __forceinline__ void btree_o_bad(Ctrl *ctrl) { atomicOr(&ctrl->error, 1u << TL_ERROR_UNSUPPORTED); }
+
+// Plan O: tile u's ticket.
+TL_HD uint32_t btree_o_rank(const BtreeStream &S, uint64_t u) { return ld_entry(S.tab + u).x; }
+
+// Plan O: may a key of source tile `own` be stored straight into tile u?
+TL_HD bool btree_o_direct(const BtreeStream &S, uint64_t own, uint64_t u) {
+    return u == own || btree_o_rank(S, u) < btree_o_rank(S, own);
+}
+
+// soff of a tile that owns no scratch: any store through it lands far outside
+// the scratch, so the kernels check for it (btree_o_bad) before storing.
+constexpr int64_t kNoScratch = INT64_MIN;
+
+// The scratch offset of tile u for its entry e = tab[u].
+TL_HD int64_t btree_o_soff_of(const BtreeStream &S, uint64_t u, uint2 e) {
+    return e.y == kNoSlot ? kNoScratch : ((int64_t)e.y - (int64_t)u) * (int64_t)S.tile_keys;
+}
+
+// Plan O: the offset of destination tile u's scratch slots.
+TL_HD int64_t btree_o_soff(const BtreeStream &S, uint64_t u) { return btree_o_soff_of(S, u, ld_entry(S.tab + u)); }
 
 // The division table of BtreeStream: pdiv[k] divides by (b+1)^k (k >= 1, while
 // that fits 63 bits; larger powers exceed every n and are never used).
@@ -77,7 +133,7 @@ TL_HD uint64_t btree_div_pow(const BtreeStream &S, uint64_t y, uint32_t k) {
 }
 
 TL_HD uint64_t btree_tile_of_ticket(const BtreeStream &S, uint64_t t) {
-    return S.plan == PLAN_R ? S.ntiles - 1 - t : t;
+    return S.plan == PLAN_R ? S.ntiles - 1 - t : S.plan == PLAN_O ? ld_table(S.order + t) : t;
 }
 
 // Source range of tile k (tiles ascend with position).
@@ -120,15 +176,24 @@ TL_HD uint64_t btree_top_last_dest_bound(const BtreeStream &S, uint64_t s) {
 // Tiles (other than k) whose source lies under the destinations of the tile's
 // bulk keys (plan R: its last-level keys; plan L: its keys of the top tree's
 // last level): right of the tile for plan R, left of it for plan L, i.e.
-// always tiles with earlier tickets.  False if there are none.
+// always tiles with earlier tickets.  False if there are none.  Plan O: every
+// tile under the destinations of the tile's bulk keys (last-level keys, or on a
+// tail tile its keys of the top tree's last level); the caller waits only for
+// those that take direct stores (btree_o_direct).
 TL_HD bool btree_tile_wait(const BtreeStream &S, uint64_t p0, uint64_t p1, uint64_t &k_lo, uint64_t &k_hi) {
     const BtreeGeom &g = S.g;
-    if (S.plan == PLAN_R) {
+    if (S.plan == PLAN_O && p0 >= g.lir && g.lir < g.n) {  // tail tile: its top-last-level keys are bulk
+        const uint64_t d0 = btree_top_last_dest_bound(S, p0), d1 = btree_top_last_dest_bound(S, p1 - 1) + 1;
+        k_lo = d0 >> S.tile_shift;
+        k_hi = (d1 - 1) >> S.tile_shift;
+        return true;
+    }
+    if (S.plan != PLAN_L) {
         if (p0 >= g.lir) return false;
         uint64_t d0 = btree_leaf_dest_bound(S, p0);
         uint64_t d1 = btree_leaf_dest_bound(S, (p1 < g.lir ? p1 : g.lir) - 1) + 1;
         if (d1 > g.n) d1 = g.n;  // a trailing separator bounds past the last leaf key
-        uint64_t lo = d0 > p1 ? d0 : p1;
+        uint64_t lo = S.plan == PLAN_O ? d0 : d0 > p1 ? d0 : p1;
         if (lo >= d1) return false;
         k_lo = lo >> S.tile_shift;
         k_hi = (d1 - 1) >> S.tile_shift;
@@ -146,6 +211,7 @@ TL_HD bool btree_tile_wait(const BtreeStream &S, uint64_t p0, uint64_t p1, uint6
 
 // Scratch slot of a final position that goes through scratch.
 TL_HD uint64_t btree_scratch_slot(const BtreeStream &S, uint64_t p) {
+    if (S.plan == PLAN_O) return p + (uint64_t)btree_o_soff(S, p >> S.tile_shift);
     return p < S.g.ni ? p : p - S.g.ni + S.seg1;
 }
 
@@ -153,9 +219,73 @@ TL_HD uint64_t btree_scratch_slot(const BtreeStream &S, uint64_t p) {
 // false -> scratch[idx].
 TL_HD bool btree_place(const BtreeStream &S, uint64_t x, uint64_t &idx) {
     const uint64_t p = btree_pos(S.g, S.fd, x);
-    const bool direct = p >= S.g.ni ? S.plan == PLAN_R : btree_top_direct(S, p);
+    const bool direct = S.plan == PLAN_O ? btree_o_direct(S, x >> S.tile_shift, p >> S.tile_shift)
+                        : p >= S.g.ni    ? S.plan == PLAN_R
+                                         : btree_top_direct(S, p);
     idx = direct ? p : btree_scratch_slot(S, p);
     return direct;
+}
+
+// Sorted rank of the key at layout position p (the inverse of btree_pos).  On
+// level k of the top tree the t-th position holds x = t + 1 + floor(t / b),
+// i.e. top rank c = x (b+1)^k - 1; on the last level the j-th position holds
+// full-leaf key j + floor(j / b) or, past them, partial-leaf key j + i.
+TL_HD uint64_t btree_src_rank(const BtreeStream &S, uint64_t p) {
+    const BtreeGeom &g = S.g;
+    if (p >= g.ni) {
+        const uint64_t j = p - g.ni;
+        if (j >= g.l) return j + g.i;
+        return j + (g.b == 1 ? j : S.fdb.div(j));
+    }
+    const uint32_t k = btree_level_of(g, p);
+    const uint64_t t = p - btree_level_start(g, k);
+    const uint64_t q = g.b == 1 ? t : S.fdb.div(t);
+    const uint64_t x = t + 1 + q;
+    return btree_top_rank(g, x * g.pw[k] - 1);
+}
+
+constexpr uint32_t kLastLevel = 0xFFFFFFFFu;  // level index of the B-tree's last level
+
+// First position of level lv (kLastLevel, or k < h of the top tree) whose key
+// has sorted rank >= sr, or the level's end.  Sorted rank grows with position
+// along a level, so the positions of one source tile form a run.
+TL_HD uint64_t btree_first_pos(const BtreeStream &S, uint32_t lv, uint64_t sr) {
+    const BtreeGeom &g = S.g;
+    if (lv == kLastLevel) {
+        uint64_t j;
+        if (sr >= g.l + g.i) {
+            j = sr - g.i;
+        } else {
+            uint64_t q, t;
+            S.fd.divmod(sr, q, t);
+            j = q * g.b + (t < g.b ? t : g.b);  // a separator (t = b) passes to the next leaf
+        }
+        return g.ni + (j < g.nl ? j : g.nl);
+    }
+    const uint64_t ls = btree_level_start(g, lv), le = btree_level_end(g, lv);
+    // smallest top rank c with btree_top_rank(c) >= sr: (c+1)(b+1) - 1 >= sr
+    // among the separators, c + l + r >= sr after them
+    uint64_t c = S.fd.div(sr + g.b + 1) - 1;
+    if (c >= g.i) {
+        const uint64_t lr = g.l + g.r;
+        c = sr > lr + g.i ? sr - lr : g.i;
+    }
+    // smallest x, not a multiple of b+1, with x (b+1)^lv - 1 >= c
+    const uint64_t x0 = btree_div_pow(S, c + g.pw[lv], lv);
+    uint64_t q, rem;
+    S.fd.divmod(x0, q, rem);
+    const uint64_t t = q * g.b + (rem ? rem : 1) - 1;
+    return ls + t < le ? ls + t : le;
+}
+
+// Plan O on top of a geometry, with scratch for `scratch_tiles` destination tiles.
+TL_HD void btree_set_ordered(BtreeStream &S, const uint2 *tab, const uint32_t *order, uint64_t scratch_tiles) {
+    S.plan = PLAN_O;
+    S.tab = tab;
+    S.order = order;
+    S.E = 0;
+    S.seg1 = S.g.ni;
+    S.nscratch = scratch_tiles * S.tile_keys;
 }
 
 // Is sorted rank x a key of the top tree?
@@ -277,11 +407,15 @@ struct TopGroup {
     uint32_t kmin;
 };
 
+// kind 3 (plan O, full leaves): kind 1 with targets per destination tile: bulk
+// indices below dsplit go to A when to_A, else to scratch at index + slo; the
+// others to A when hi_A, else to scratch at index + shi.
 struct Regime {
     int kind;
-    bool to_A;
+    bool to_A, hi_A;
     uint32_t r0, skip;
-    uint64_t dbase;
+    uint64_t dbase, dsplit;
+    int64_t slo, shi;
 };
 
 TL_HD TopGroup btree_sep_group(const BtreeStream &S, uint64_t p0, uint64_t end) {
@@ -305,6 +439,24 @@ TL_HD TopGroup btree_tail_group(const BtreeStream &S, uint64_t p0, uint64_t star
     return G;
 }
 
+// Plan O: a kind-1 regime's bulk indices start at that of its first non-skip
+// offset and span fewer than tile_keys positions, i.e. at most two destination
+// tiles; kind 3 splits them there.
+TL_HD void btree_regime_split(const BtreeStream &S, uint64_t p0, Regime &R) {
+    const uint32_t d = (uint32_t)S.g.b + 1;
+    const uint32_t v0 = R.r0 == R.skip ? R.r0 + 1 : R.r0;
+    const uint64_t own = p0 >> S.tile_shift, u0 = (R.dbase + v0 - v0 / d) >> S.tile_shift;
+    R.kind = 3;
+    R.dsplit = (u0 + 1) << S.tile_shift;
+    const bool two = u0 + 1 < S.ntiles;
+    const uint32_t ro = btree_o_rank(S, own);
+    const uint2 e0 = ld_entry(S.tab + u0), e1 = two ? ld_entry(S.tab + u0 + 1) : make_uint2(0, kNoSlot);
+    R.to_A = u0 == own || e0.x < ro;
+    R.hi_A = !two || u0 + 1 == own || e1.x < ro;
+    R.slo = R.to_A ? 0 : btree_o_soff_of(S, u0, e0);
+    R.shi = R.hi_A ? 0 : btree_o_soff_of(S, u0 + 1, e1);
+}
+
 TL_HD Regime btree_stream_regime(const BtreeStream &S, uint64_t p0, uint64_t p1) {
     const BtreeGeom &g = S.g;
     Regime R{};
@@ -315,8 +467,9 @@ TL_HD Regime btree_stream_regime(const BtreeStream &S, uint64_t p0, uint64_t p1)
         R.kind = 1;
         R.r0 = (uint32_t)r0;
         R.skip = (uint32_t)g.b;
-        R.to_A = S.plan == PLAN_R;
+        R.to_A = S.plan != PLAN_L;
         R.dbase = R.to_A ? g.ni + q0 * g.b : S.seg1 + q0 * g.b;
+        if (S.plan == PLAN_O) btree_regime_split(S, p0, R);
     } else if (p0 >= g.lir) {  // trailing top keys
         if (S.plan == PLAN_R) {
             R.kind = 2;
@@ -327,13 +480,14 @@ TL_HD Regime btree_stream_regime(const BtreeStream &S, uint64_t p0, uint64_t p1)
             R.skip = 0;
             R.to_A = true;
             R.dbase = S.i2 + q0 * g.b - 1;
+            if (S.plan == PLAN_O) btree_regime_split(S, p0, R);
         }
     }
     return R;
 }
 
 // The tile's groups of top keys (levels kmin.. of each); returns their number.
-// Under plan L a tail tile's keys of the top tree's last level are bulk keys.
+// Under plans L and O a tail tile's keys of the top tree's last level are bulk keys.
 TL_HD int btree_stream_groups(const BtreeStream &S, uint64_t p0, uint64_t p1, TopGroup &G0, TopGroup &G1) {
     const BtreeGeom &g = S.g;
     if (g.h == 0) return 0;
@@ -368,6 +522,19 @@ TL_HD bool btree_regime_bulk(const BtreeStream &S, const Regime &R, uint32_t o, 
     return true;
 }
 
+// Kind 3: every part of the bulk range that goes to scratch has scratch.
+TL_HD bool btree_regime_ok(const BtreeStream &S, const Regime &R, uint32_t cnt) {
+    const uint32_t d = S.fd32.d;
+    uint32_t v0 = R.r0, v1 = R.r0 + cnt - 1;  // first and last bulk offsets (+ r0)
+    if (v0 % d == R.skip) ++v0;
+    if (v1 % d == R.skip) --v1;
+    if (cnt == 0 || v0 > v1) return true;
+    const uint64_t i0 = R.dbase + v0 - v0 / d, i1 = R.dbase + v1 - v1 / d;
+    if (i0 < R.dsplit && !R.to_A && R.slo == kNoScratch) return false;
+    if (i1 >= R.dsplit && !R.hi_A && R.shi == kNoScratch) return false;
+    return true;
+}
+
 // One level's run of top keys inside a tile.  Level k holds the top ranks with
 // c + 1 = x (b+1)^k, x not a multiple of b+1; the t-th such x (t counted from 0
 // over the whole level) is x = t + 1 + floor(t / b) and lands at
@@ -376,11 +543,15 @@ TL_HD bool btree_regime_bulk(const BtreeStream &S, const Regime &R, uint32_t o, 
 // remainder mod b+1, and sits at tile offset x * mult - gneg (mult = (b+1)^k f),
 // i.e. off0 + (e + floor((rb + e) / b)) * mult with off0 = xb * mult - gneg.
 // Offsets are below the tile size, so they are computed modulo 2^32.  Elements
-// [0, nlo) of the run (positions below bnd[k]) go to A under plan R and to
-// scratch under plan L, the rest the other way round.
+// [0, nlo) of the run go to A when bit 0 of `direct` is set, the rest when bit
+// 1 is; otherwise to scratch, at the position (plans R, L) or at the position +
+// slo / shi (plan O).  Under plan R nlo splits at bnd[k] with direct = 1, under
+// plan L with direct = 2; under plan O nlo is where the run crosses into the
+// next destination tile.
 struct TopRun {
     uint64_t dest0;
-    uint32_t off0, mult, rb, cnt, nlo, pad;
+    int64_t slo, shi;
+    uint32_t off0, mult, rb, cnt, nlo, direct;
 };
 
 // The run of level k of a group of top keys (cnt = 0 when empty).  With hi_k =
@@ -389,7 +560,7 @@ struct TopRun {
 // or below lo_k, and (hi_k - hi_{k+1}) - t0 in the range (hi_{k+1} =
 // floor(hi_k / (b+1))).  A tile's runs occupy slots s = group * kMaxTopLevels +
 // level; slots of levels below kmin or above the tree are empty.
-TL_HD TopRun btree_group_run(const BtreeStream &S, const TopGroup &G, uint32_t k) {
+TL_HD TopRun btree_group_run(const BtreeStream &S, const TopGroup &G, uint32_t k, uint64_t own) {
     const BtreeGeom &g = S.g;
     TopRun run{};
     if (k < G.kmin || k >= g.h || G.y_lo > G.y_hi) return run;
@@ -411,71 +582,112 @@ TL_HD TopRun btree_group_run(const BtreeStream &S, const TopGroup &G, uint32_t k
     const uint64_t mult = g.pw[k] * G.f;
     run.mult = (uint32_t)mult;
     run.off0 = (uint32_t)(xb * mult - G.gneg);
+    if (S.plan == PLAN_O) {  // a run spans fewer than tile_keys positions: at most two tiles
+        const uint64_t u0 = run.dest0 >> S.tile_shift, split = (u0 + 1) << S.tile_shift;
+        run.nlo = split - run.dest0 < run.cnt ? (uint32_t)(split - run.dest0) : run.cnt;
+        const bool two = run.nlo < run.cnt;
+        const uint32_t ro = btree_o_rank(S, own);
+        const uint2 e0 = ld_entry(S.tab + u0), e1 = two ? ld_entry(S.tab + u0 + 1) : make_uint2(0, kNoSlot);
+        const bool d0 = u0 == own || e0.x < ro, d1 = two && (u0 + 1 == own || e1.x < ro);
+        run.direct = (d0 ? 1u : 0u) | (d1 ? 2u : 0u);
+        if (!d0) run.slo = btree_o_soff_of(S, u0, e0);
+        if (two && !d1) run.shi = btree_o_soff_of(S, u0 + 1, e1);
+        return run;
+    }
     const uint64_t bk = S.bnd[k];
     run.nlo = bk <= run.dest0 ? 0 : (bk - run.dest0 < run.cnt ? (uint32_t)(bk - run.dest0) : run.cnt);
+    run.direct = S.plan == PLAN_R ? 1u : 2u;
     return run;
 }
 
+
 // Tile offset of element e of a run.
-TL_HD uint32_t btree_top_item_off(const BtreeStream &S, const TopRun &run, uint32_t e) {
+template <class Run>
+TL_HD uint32_t btree_top_item_off(const BtreeStream &S, const Run &run, uint32_t e) {
     const uint32_t qe = S.g.b == 1 ? e : S.fd32b.div(run.rb + e);  // b = 1: rb = 0
     return run.off0 + (e + qe) * run.mult;
 }
 
 // Does element e of a run go straight to A?
 TL_HD bool btree_run_direct(const BtreeStream &S, const TopRun &run, uint32_t e) {
-    return (e < run.nlo) == (S.plan == PLAN_R);
+    return (run.direct >> (e < run.nlo ? 0 : 1)) & 1u;
 }
 
 // Tiles under the direct part of a run (all with earlier tickets, or the tile
 // itself); false when the run has no direct part.
 TL_HD bool btree_run_wait(const BtreeStream &S, const TopRun &run, uint64_t &k_lo, uint64_t &k_hi) {
-    const bool lo_direct = S.plan == PLAN_R;
-    const uint32_t e0 = lo_direct ? 0 : run.nlo, e1 = lo_direct ? run.nlo : run.cnt;
+    const uint32_t e0 = (run.direct & 1u) ? 0 : run.nlo, e1 = (run.direct & 2u) ? run.cnt : run.nlo;
     if (e0 >= e1) return false;
     k_lo = (run.dest0 + e0) >> S.tile_shift;
     k_hi = (run.dest0 + e1 - 1) >> S.tile_shift;
     return true;
 }
 
-// Shared-memory workspace of btree_stream_tile.
-struct TileShared {
-    TopRun runs[kMaxTopRuns];
-    uint32_t cum[kMaxTopRuns + 1];
-    uint32_t nslots;
-    int ok;
+// What the block's store loop needs of a run: for element e, the key at tile
+// offset btree_top_item_off goes to (e < nlo ? blo : bhi)[e], the two bases
+// being the run's first destination in A or in the scratch.
+struct StoreRun {
+    uint64_t blo, bhi;
+    uint32_t off0, mult, rb, nlo;
 };
 
-// Warp 0's part of btree_stream_tile: the tile's runs (one lane per slot), their
-// prefix sums, and the waits for the tiles under their direct parts.  Kept out
-// of line so that its 64-bit state does not crowd the registers of the tile loops.
+// Shared-memory workspace of btree_stream_tile.
+struct TileShared {
+    StoreRun runs[kMaxTopRuns];
+    uint32_t cum[kMaxTopRuns + 1];
+    uint32_t nslots;
+    int ok0, ok1;  // warp 0's and warps 1..'s waits all ended (and no schedule error)
+    Regime reg;
+};
+
+// Warp 0's part of btree_stream_tile: the tile's runs (one lane per slot, a
+// slot per level of each group of top keys, with their plan-O table lookups),
+// their prefix sums and store bases, and the waits for the tiles under their
+// direct parts.  Kept out of line so that its 64-bit state does not crowd the
+// registers of the tile loops.
 static __device__ __noinline__ void btree_tile_runs_warp(const BtreeStream &S, uint64_t p0, uint64_t p1,
-                                                  unsigned int *flags, Ctrl *ctrl, const WaitCfg &wc,
-                                                  TileShared &ts) {
+                                                         uintptr_t ab, uintptr_t sb, uint32_t kb,
+                                                         unsigned int *flags, Ctrl *ctrl, const WaitCfg &wc,
+                                                         TileShared &ts) {
     const uint32_t lane = threadIdx.x;
+    const uint64_t own = p0 >> S.tile_shift;
     TopGroup G0{}, G1{};
     const int ng = btree_stream_groups(S, p0, p1, G0, G1);
-    const uint32_t nslots = (uint32_t)ng * kMaxTopLevels;
+    const uint32_t h = S.g.h, nslots = (uint32_t)ng * h;  // slot = group * h + level
     uint32_t carry = 0;
     for (uint32_t s0 = 0; s0 < nslots; s0 += 32) {
         const uint32_t sl = s0 + lane;
         TopRun run{};
-        if (sl < nslots) run = btree_group_run(S, sl < kMaxTopLevels ? G0 : G1, sl % kMaxTopLevels);
+        if (sl < nslots) run = btree_group_run(S, sl < h ? G0 : G1, sl < h ? sl : sl - h, own);
         uint32_t incl = run.cnt;
 #pragma unroll
         for (int dd = 1; dd < 32; dd <<= 1) {
             const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, dd);
             if (lane >= (uint32_t)dd) incl += y;
         }
+        if (S.plan == PLAN_O && run.cnt &&
+            ((run.nlo && !(run.direct & 1u) && run.slo == kNoScratch) ||
+             (run.nlo < run.cnt && !(run.direct & 2u) && run.shi == kNoScratch))) {
+            btree_o_bad(ctrl);
+            ts.ok0 = 0;
+        }
         if (sl < nslots) {
-            ts.runs[sl] = run;
+            StoreRun sr;
+            const uintptr_t d0 = (uintptr_t)run.dest0 * kb;
+            sr.blo = (run.direct & 1u) ? ab + d0 : sb + d0 + (uintptr_t)run.slo * kb;
+            sr.bhi = (run.direct & 2u) ? ab + d0 : sb + d0 + (uintptr_t)run.shi * kb;
+            sr.off0 = run.off0;
+            sr.mult = run.mult;
+            sr.rb = run.rb;
+            sr.nlo = run.nlo;
+            ts.runs[sl] = sr;
             ts.cum[sl] = carry + incl - run.cnt;
         }
         carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
         uint64_t r_lo, r_hi;
         if (run.cnt && btree_run_wait(S, run, r_lo, r_hi))
             for (uint64_t f = r_lo; f <= r_hi; ++f)
-                if (!wait_flag(&flags[f], wc.wait_value, ctrl, wc)) ts.ok = 0;
+                if (!wait_flag(&flags[f], wc.wait_value, ctrl, wc)) ts.ok0 = 0;
     }
     if (lane == 0) {
         ts.cum[nslots] = carry;
@@ -489,32 +701,46 @@ __device__ __forceinline__ void bar_sync_tail() {
 }
 
 // Stream pass for tile k of one array (block-wide).  False if a bounded wait
-// expired (the tile's stores were skipped and the error is recorded).  Warp 0
-// computes the tile's runs of top keys (one lane per level) and waits for the
-// tiles under their direct parts, while warps 1.. wait for the tiles under the
-// bulk keys and store those; then the whole block stores the top keys.
+// expired (the tile's stores were skipped and the error is recorded).  Warps
+// 1.. load the tile, publish it and store its bulk keys (after waiting for the
+// tiles under them); meanwhile warp 0 computes the tile's runs of top keys (one
+// lane per level, with their table lookups) and waits for the tiles under
+// their direct parts, so that its work stays off the load's path.  Then the
+// whole block stores the top keys.  Every wait is on a tile with an earlier
+// ticket, and the publish does not depend on warp 0.
 template <typename K>
 __device__ __forceinline__ bool btree_stream_tile(const BtreeStream &S, K *__restrict__ A, K *__restrict__ scr,
                                                   unsigned int *flags, Ctrl *ctrl, const WaitCfg &wc, uint64_t k,
                                                   K *sm, TileShared &ts) {
     uint64_t p0, p1;
     btree_tile(S, k, p0, p1);
-    if (threadIdx.x == 0) ts.ok = 1;  // the previous tile's readers are past the ticket barrier
-    const uint64_t base = load_tile(A, p0, p1, sm);
-    publish_read(&flags[k], wc);
+    const uint64_t base = tile_base(A, p0);
     const uint32_t cnt = (uint32_t)(p1 - p0);
     const K *tile = sm + (p0 - base);
     if (threadIdx.x < 32) {
-        btree_tile_runs_warp(S, p0, p1, flags, ctrl, wc, ts);
+        if (threadIdx.x == 0) ts.ok0 = 1;  // the previous tile's readers are past the ticket barrier
+        __syncwarp();
+        btree_tile_runs_warp(S, p0, p1, reinterpret_cast<uintptr_t>(A), reinterpret_cast<uintptr_t>(scr),
+                             (uint32_t)sizeof(K), flags, ctrl, wc, ts);
     } else {
         const uint32_t tb = threadIdx.x - 32, nb = blockDim.x - 32;
+        if (tb == 0) {
+            ts.ok1 = 1;
+            ts.reg = btree_stream_regime(S, p0, p1);
+        }
+        load_tile_issue(A, p0, p1, sm, tb, nb);
+        load_tile_wait();
+        bar_sync_tail();  // the tile is in shared memory
+        if (tb == 0) st_relaxed(&flags[k], wc.flag_value);  // published: every copy has landed
         uint64_t w_lo, w_hi;
         if (btree_tile_wait(S, p0, p1, w_lo, w_hi))
-            for (uint64_t f = w_lo + tb; f <= w_hi; f += nb)
-                if (!wait_flag(&flags[f], wc.wait_value, ctrl, wc)) ts.ok = 0;
+            for (uint64_t f = w_lo + tb; f <= w_hi; f += nb) {
+                if (S.plan == PLAN_O && !btree_o_direct(S, k, f)) continue;  // its keys go to scratch
+                if (!wait_flag(&flags[f], wc.wait_value, ctrl, wc)) ts.ok1 = 0;
+            }
         bar_sync_tail();
-        if (ts.ok) {
-            const Regime R = btree_stream_regime(S, p0, p1);
+        if (ts.ok1) {
+            const Regime &R = ts.reg;  // fields read from shared memory where used
             if (R.kind == 0) {
                 for (uint64_t x = p0 + tb; x < p1; x += nb) {
                     if (btree_is_top(S, x)) continue;
@@ -522,34 +748,227 @@ __device__ __forceinline__ bool btree_stream_tile(const BtreeStream &S, K *__res
                     const K key = sm[x - base];
                     if (btree_place(S, x, idx))
                         A[idx] = key;
-                    else
+                    else if (idx < S.nscratch)
                         scr[idx] = key;
+                    else
+                        btree_o_bad(ctrl);
                 }
             } else if (R.kind == 1) {
-                K *tgt = R.to_A ? A : scr;
-                const uint32_t d = S.fd32.d;
+                // the loops keep the regime in registers (stores through K * could alias it)
+                K *tgt = (R.to_A ? A : scr) + R.dbase;
+                const uint32_t d = S.fd32.d, r0 = R.r0, skip = R.skip;
 #pragma unroll 4
                 for (uint32_t o = tb; o < cnt; o += nb) {
-                    const uint32_t v = R.r0 + o;
+                    const uint32_t v = r0 + o;
                     const uint32_t ql = S.fd32.div(v);
-                    if (v - ql * d != R.skip) tgt[R.dbase + (v - ql)] = tile[o];
+                    if (v - ql * d != skip) tgt[v - ql] = tile[o];
+                }
+            } else if (R.kind == 3 && !btree_regime_ok(S, R, cnt)) {
+                if (tb == 0) btree_o_bad(ctrl);
+            } else if (R.kind == 3) {
+                K *tlo = (R.to_A ? A : scr + R.slo) + R.dbase, *thi = (R.hi_A ? A : scr + R.shi) + R.dbase;
+                const uint32_t d = S.fd32.d, r0 = R.r0, skip = R.skip;
+                const uint32_t split = (uint32_t)(R.dsplit - R.dbase);  // below tile_keys + b
+#pragma unroll 4
+                for (uint32_t o = tb; o < cnt; o += nb) {
+                    const uint32_t v = r0 + o;
+                    const uint32_t ql = S.fd32.div(v);
+                    const uint32_t j = v - ql;
+                    if (v - ql * d != skip) (j < split ? tlo : thi)[j] = tile[o];
                 }
             }
         }
     }
     __syncthreads();
-    if (!ts.ok) return false;
+    if (!ts.ok0 || !ts.ok1) return false;
     // top keys, level by level: consecutive threads store consecutive positions
     const uint32_t total = ts.cum[ts.nslots];
     uint32_t r = 0;  // the run of gi only moves forward as gi grows
     for (uint32_t gi = threadIdx.x; gi < total; gi += blockDim.x) {
         while (gi >= ts.cum[r + 1]) ++r;
-        const TopRun run = ts.runs[r];
+        const StoreRun run = ts.runs[r];
         const uint32_t e = gi - ts.cum[r];
-        K *dst = btree_run_direct(S, run, e) ? A : scr;
-        dst[run.dest0 + e] = tile[btree_top_item_off(S, run, e)];
+        K *dst = reinterpret_cast<K *>(e < run.nlo ? run.blo : run.bhi);
+        dst[e] = tile[btree_top_item_off(S, run, e)];
     }
     return true;
+}
+
+// ---------------------------------------------------------------- plan O second pass
+// Destination tile u's positions split into one piece per level; along a piece
+// the source tiles z0..z1 of its keys come in runs of consecutive positions
+// (btree_first_pos).  The run of source tile z went to scratch iff z != u and
+// rank[z] < rank[u] (z was processed before u was read).
+
+// The piece of tile u's positions that starts at position a: its level and end.
+TL_HD void btree_fix_piece(const BtreeStream &S, uint64_t a, uint64_t P1, uint32_t &lv, uint64_t &e) {
+    const BtreeGeom &g = S.g;
+    if (a >= g.ni) {
+        lv = kLastLevel;
+        e = P1;
+        return;
+    }
+    lv = btree_level_of(g, a);
+    const uint64_t le = btree_level_end(g, lv);
+    e = le < P1 ? le : P1;
+}
+
+// Positions [pa, pe) of source tile z within the piece [a, e) of level lv whose
+// source tiles run from z0 to z1.
+TL_HD void btree_fix_run(const BtreeStream &S, uint32_t lv, uint64_t a, uint64_t e, uint64_t z0, uint64_t z1,
+                         uint64_t z, uint64_t &pa, uint64_t &pe) {
+    pa = z == z0 ? a : btree_first_pos(S, lv, z << S.tile_shift);
+    pe = z == z1 ? e : btree_first_pos(S, lv, (z + 1) << S.tile_shift);
+    if (pa < a) pa = a;
+    if (pe > e) pe = e;
+    if (pe < pa) pe = pa;
+}
+
+// Sorted rank of position p on level lv (kLastLevel or a top level): the
+// inverse of btree_pos without the level search.
+TL_HD uint64_t btree_src_rank_at(const BtreeStream &S, uint32_t lv, uint64_t p) {
+    const BtreeGeom &g = S.g;
+    if (lv == kLastLevel) {
+        const uint64_t j = p - g.ni;
+        return j >= g.l ? j + g.i : j + (g.b == 1 ? j : S.fdb.div(j));
+    }
+    const uint64_t t = p - btree_level_start(g, lv);
+    const uint64_t x = t + 1 + (g.b == 1 ? t : S.fdb.div(t));
+    return btree_top_rank(g, x * g.pw[lv] - 1);
+}
+
+// Host form (replay, scratch lists and counts): calls visit(pa, len) for each
+// scratch run of tile u (positions; u's slots are at position + soff[u]) until
+// visit returns false.  Same two cases as the device form below: a piece with
+// few source tiles by source runs, any other position by position.
+template <class Visit>
+__host__ void btree_fix_tile_host(const BtreeStream &S, uint64_t u, Visit &&visit);
+
+// Device form, one warp per tile.  A piece with few source tiles (at most
+// kFixDense) has long runs: the lanes find them, one per lane, and the warp
+// copies them with consecutive lanes on consecutive keys - as one range when
+// the scratch runs of the lanes are contiguous (the common case: whole levels
+// go through scratch), else run by run.  A piece whose keys come from more tiles
+// than that (a level high in the tree, whose consecutive positions draw on
+// distant tiles) is walked position by position.
+constexpr int kFixUnr = 8;
+constexpr uint64_t kFixDense = 64;
+
+// The warp copies src[lo, hi) to dst[lo, hi), kFixUnr keys per lane in flight.
+template <typename K>
+__device__ __forceinline__ void warp_copy_keys(K *__restrict__ dst, const K *__restrict__ src, uint32_t lo,
+                                               uint32_t hi) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t q = lo; q < hi; q += 32 * kFixUnr) {
+        K v[kFixUnr];
+#pragma unroll
+        for (int r = 0; r < kFixUnr; ++r) {
+            const uint32_t x = q + r * 32 + lane;
+            if (x < hi) v[r] = __ldcs(src + x);
+        }
+#pragma unroll
+        for (int r = 0; r < kFixUnr; ++r) {
+            const uint32_t x = q + r * 32 + lane;
+            if (x < hi) dst[x] = v[r];
+        }
+    }
+}
+
+template <typename K>
+__device__ __forceinline__ void btree_fix_tile_warp(const BtreeStream &S, K *__restrict__ A,
+                                                    const K *__restrict__ scr, uint64_t u) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t P0 = u << S.tile_shift, P1 = P0 + S.tile_keys < S.g.n ? P0 + S.tile_keys : S.g.n;
+    const uint32_t ru = btree_o_rank(S, u);
+    // the tile's positions and its scratch, indexed from the tile start
+    K *At = A + P0;
+    const K *St = scr + btree_o_soff(S, u) + P0;
+    for (uint64_t a = P0; a < P1;) {
+        uint32_t lv;
+        uint64_t e;
+        btree_fix_piece(S, a, P1, lv, e);
+        const uint64_t z0 = btree_src_rank_at(S, lv, a) >> S.tile_shift;
+        const uint64_t z1 = btree_src_rank_at(S, lv, e - 1) >> S.tile_shift;
+        if (z1 - z0 < kFixDense) {
+            for (uint64_t zb = z0; zb <= z1; zb += 32) {
+                const uint64_t z = zb + lane;
+                uint64_t pa = 0, pe = 0;
+                if (z <= z1 && z != u && btree_o_rank(S, z) < ru) btree_fix_run(S, lv, a, e, z0, z1, z, pa, pe);
+                const uint32_t len = (uint32_t)(pe - pa);
+                const uint32_t lo = len ? (uint32_t)(pa - P0) : 0xFFFFFFFFu, hi = len ? (uint32_t)(pe - P0) : 0;
+                const uint32_t rlo = __reduce_min_sync(0xFFFFFFFFu, lo), rhi = __reduce_max_sync(0xFFFFFFFFu, hi);
+                const uint32_t sum = __reduce_add_sync(0xFFFFFFFFu, len);
+                if (sum == 0) continue;
+                if (sum == rhi - rlo) {  // the lanes' runs tile [rlo, rhi)
+                    warp_copy_keys(At, St, rlo, rhi);
+                    continue;
+                }
+                uint32_t todo = __ballot_sync(0xFFFFFFFFu, len != 0);
+                while (todo) {
+                    const int j = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    warp_copy_keys(At, St, __shfl_sync(0xFFFFFFFFu, lo, j), __shfl_sync(0xFFFFFFFFu, hi, j));
+                }
+            }
+        } else {
+            const uint32_t ea = (uint32_t)(a - P0), ee = (uint32_t)(e - P0);
+            for (uint32_t q = ea; q < ee; q += 32 * kFixUnr) {
+                bool take[kFixUnr];
+                K v[kFixUnr];
+#pragma unroll
+                for (int r = 0; r < kFixUnr; ++r) {
+                    const uint32_t x = q + r * 32 + lane;
+                    take[r] = false;
+                    if (x < ee) {
+                        const uint64_t z = btree_src_rank_at(S, lv, P0 + x) >> S.tile_shift;
+                        take[r] = z != u && btree_o_rank(S, z) < ru;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kFixUnr; ++r)
+                    if (take[r]) v[r] = __ldcs(St + q + r * 32 + lane);
+#pragma unroll
+                for (int r = 0; r < kFixUnr; ++r)
+                    if (take[r]) At[q + r * 32 + lane] = v[r];
+            }
+        }
+        a = e;
+    }
+}
+
+template <class Visit>
+__host__ void btree_fix_tile_host(const BtreeStream &S, uint64_t u, Visit &&visit) {
+    const uint64_t P0 = u << S.tile_shift, P1 = P0 + S.tile_keys < S.g.n ? P0 + S.tile_keys : S.g.n;
+    const uint32_t ru = btree_o_rank(S, u);
+    for (uint64_t a = P0; a < P1;) {
+        uint32_t lv;
+        uint64_t e;
+        btree_fix_piece(S, a, P1, lv, e);
+        const uint64_t z0 = btree_src_rank_at(S, lv, a) >> S.tile_shift;
+        const uint64_t z1 = btree_src_rank_at(S, lv, e - 1) >> S.tile_shift;
+        if (z1 - z0 < kFixDense) {
+            for (uint64_t z = z0; z <= z1; ++z) {
+                if (z == u || btree_o_rank(S, z) > ru) continue;
+                uint64_t pa, pe;
+                btree_fix_run(S, lv, a, e, z0, z1, z, pa, pe);
+                if (pe > pa && !visit(pa, pe - pa)) return;
+            }
+        } else {
+            uint64_t run0 = 0, len = 0;
+            for (uint64_t x = a; x < e; ++x) {
+                const uint64_t z = btree_src_rank_at(S, lv, x) >> S.tile_shift;
+                if (z != u && btree_o_rank(S, z) < ru) {
+                    if (!len) run0 = x;
+                    ++len;
+                } else if (len) {
+                    if (!visit(run0, len)) return;
+                    len = 0;
+                }
+            }
+            if (len && !visit(run0, len)) return;
+        }
+        a = e;
+    }
 }
 
 // Second pass: the scratch ranges still to copy into place.  Range j < h: the
@@ -560,7 +979,7 @@ struct CopyRange {
     uint64_t dst, src, len;
 };
 
-TL_HD int btree_copy_range_count(const BtreeStream &S) { return (int)S.g.h + 1; }
+TL_HD int btree_copy_range_count(const BtreeStream &S) { return S.plan == PLAN_O ? 0 : (int)S.g.h + 1; }
 
 TL_HD bool btree_copy_range(const BtreeStream &S, int j, CopyRange &r) {
     const BtreeGeom &g = S.g;

@@ -7,6 +7,7 @@
 #include "geometry.cuh"
 #include "internal.h"
 #include "learned.h"
+#include "stream.cuh"
 #include "batched.h"
 
 namespace tl {
@@ -28,6 +29,18 @@ int read_error_word(const unsigned int *dev_word, unsigned int *out, cudaStream_
     TL_CUDA_TRY(cudaMemcpyAsync(out, dev_word, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
     TL_CUDA_TRY(cudaStreamSynchronize(st));
     return TL_SUCCESS;
+}
+
+// Wait statistics of the last permutation (test and profiling hook).
+static std::atomic<unsigned long long> g_stalled_waits{0}, g_stall_polls{0};
+
+void record_wait_stats(const Ctrl *ctrl, cudaStream_t st) {
+    unsigned long long v[2] = {0, 0};
+    if (cudaMemcpyAsync(v, &ctrl->stalled_waits, sizeof v, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return;
+    g_stalled_waits = v[0];
+    g_stall_polls = v[1];
 }
 
 int sync_and_check(cudaStream_t st) {
@@ -118,9 +131,28 @@ int tl_debug_struct_size(int which) {
     }
 }
 
-// Test hook: which B-tree schedule the permutation uses (0: right-to-left
-// stream, top tree via scratch; 1: left-to-right stream, last level via scratch).
+// Test hook: which fixed-direction B-tree schedule the permutation uses (0:
+// right-to-left stream, top tree via scratch; 1: left-to-right stream, last
+// level via scratch).
 int tl_debug_btree_plan(uint64_t n, uint64_t b) { return btree_plan_of(n, b); }
+
+int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes) {
+    return permute_plan_of(layout, n, b, key_bytes);
+}
+
+int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes) { return stream_blocks_per_sm(layout, key_bytes); }
+
+int tl_debug_set_schedule(int fixed_only) {
+    set_fixed_schedule_only(fixed_only != 0);
+    return TL_SUCCESS;
+}
+
+int tl_debug_wait_stats(uint64_t *stalled_waits, uint64_t *polls) {
+    if (!stalled_waits || !polls) return TL_ERROR_INVALID_VALUE;
+    *stalled_waits = g_stalled_waits;
+    *polls = g_stall_polls;
+    return TL_SUCCESS;
+}
 
 int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys) {
     return permute_scratch_keys(layout, n, b, key_bytes, keys);

@@ -82,13 +82,22 @@ class EventTimer {
 // Reads a device word written by the preceding work on `st` (blocks the host).
 int read_error_word(const unsigned int *dev_word, unsigned int *out, cudaStream_t st);
 int sync_and_check(cudaStream_t st);
+struct Ctrl;
+// Keeps the wait statistics of a permutation's control block (tl_debug_wait_stats).
+void record_wait_stats(const Ctrl *ctrl, cudaStream_t st);
 
 int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
+// The workspace of the fixed-direction schedules (what permute needs when told
+// not to take the ordered one).
+int permute_workspace_bytes_fixed(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
 int btree_plan_of(uint64_t n, uint64_t b);
+int permute_plan_of(int layout, uint64_t n, uint64_t b, uint32_t key_bytes);
+void set_fixed_schedule_only(bool on);
+int stream_blocks_per_sm(int layout, uint32_t key_bytes);
 int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
 int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations);
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
-            uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms = nullptr);
+            uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms = nullptr, bool allow_ordered = true);
 
 enum QueryLayout { Q_BST = 0, Q_BTREE = 1, Q_VEB = 2, Q_VEB_NP = 3, Q_SORTED = 4 };
 struct QueryArgs {

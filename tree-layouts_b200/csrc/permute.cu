@@ -11,19 +11,22 @@
 //     into shared memory, flagged as read, and its bulk keys are stored
 //     straight to their final positions once the tiles under those positions
 //     have been read.  The other keys go to a scratch buffer.
-//  2. B-tree: a copy of the scratch (indexed by final position) into place;
-//     mvEB: a scatter of the scratch slots to their final positions.  Every
-//     destination is free by then.
+//  2. B-tree: a copy of the scratch (indexed by final position) into place,
+//     or under the ordered-tile schedule the fix pass over the tiles that
+//     received scratch keys; mvEB: a scatter of the scratch slots to their
+//     final positions.  Every destination is free by then.
 //
-// DRAM traffic is 2*n*w for the stream plus 2*w per scratch key: n/(b+1) for a
-// perfect B-tree, about n/2^8 for an mvEB.
+// DRAM traffic is 2*n*w for the stream plus 2*w per scratch key: 6-20 % of the
+// keys of a B-tree or BST under the ordered schedule, about n/2^8 for an mvEB.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
 
+#include "btree_order.h"
 #include "btree_plan.cuh"
 #include "bulk.cuh"
 #include "geometry.cuh"
@@ -67,6 +70,17 @@ btree_copy_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_con
     extern __shared__ __align__(128) unsigned char stage[];
     __shared__ __align__(8) uint64_t bars[kBulkStages];
     bulk_copy_plan(A, scr, P, stage, bars, ctrl);
+}
+
+// Second pass of a plan-O B-tree permutation: one warp per destination tile
+// that receives scratch keys (list[0, nlist)).
+template <typename K>
+__global__ void __launch_bounds__(kScatterThreads)
+btree_fix_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_constant__ BtreeStream S,
+                 const uint32_t *__restrict__ list, uint64_t nlist) {
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w; i < nlist; i += nw) btree_fix_tile_warp(S, A, scr, (uint64_t)__ldg(list + i));
 }
 
 // The copy ranges split for the bulk engine: each range's 16-byte-aligned
@@ -256,12 +270,25 @@ struct PermutePlan {
     uint32_t key_bytes = 8;
     uint64_t n = 0, b = 1;
     uint64_t tile_keys = 0, ntiles = 0, scratch_keys = 0;
+    bool ordered = false;  // B-tree plan O, with these tables (host, then device pointers)
+    OrderTables ot;
     BtreeStream bs;
     MvebParams mp;
     uint64_t off_flags = 0, off_ctrl = 0, bytes = 0;
 };
 
-static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, PermutePlan &pl) {
+// When a B-tree permutation takes plan O: ORDER_AUTO from kOrderMinTiles tiles
+// up (below that a tile order has too few tiles to pay for its second pass),
+// ORDER_ALWAYS whenever there is a top tree and more than one tile (host replay).
+enum OrderMode { ORDER_NEVER = 0, ORDER_AUTO = 1, ORDER_ALWAYS = 2 };
+constexpr uint64_t kOrderMinTiles = 64;
+static std::atomic<int> g_fixed_only{0};  // tl_debug_set_schedule: ORDER_AUTO acts as ORDER_NEVER
+
+void set_fixed_schedule_only(bool on) { g_fixed_only = on ? 1 : 0; }
+
+// Plan O's tables come from the library's cache unless `tables` are given.
+static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, PermutePlan &pl,
+                     int order_mode = ORDER_AUTO, const OrderTables *tables = nullptr) {
     if (key_bytes != 4 && key_bytes != 8) return TL_ERROR_INVALID_VALUE;
     if (layout == TL_LAYOUT_BST) b = 1;
     if (layout == TL_LAYOUT_BTREE && b == 0) return TL_ERROR_INVALID_VALUE;
@@ -284,13 +311,25 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
         if (pl.bs.g.h > (uint32_t)kMaxTopLevels || n / pl.tile_keys >= (1ull << 32)) return TL_ERROR_UNSUPPORTED;
         pl.bs.fd = FastDiv64(b + 1);
         pl.bs.fd32 = FastDiv32((uint32_t)(b + 1));
-        if (b >= 2) pl.bs.fd32b = FastDiv32((uint32_t)b);
+        if (b >= 2) {
+            pl.bs.fd32b = FastDiv32((uint32_t)b);
+            pl.bs.fdb = FastDiv64(b);
+        }
         pl.bs.tile_keys = pl.tile_keys;
         pl.bs.tile_shift = (uint32_t)__builtin_ctzll(pl.tile_keys);
         btree_set_pow_divs(pl.bs, make_pow_divs(b));
         pl.ntiles = (n + pl.tile_keys - 1) / pl.tile_keys;
         pl.bs.ntiles = pl.ntiles;
         btree_choose_plan(pl.bs, key_bytes);
+        if (pl.bs.g.h >= 1 && pl.ntiles >= 2 &&
+            (order_mode == ORDER_ALWAYS ||
+             (order_mode == ORDER_AUTO && pl.ntiles >= kOrderMinTiles && !g_fixed_only))) {
+            if (tables) pl.ot = *tables;
+            if (tables || btree_order_host(pl.bs, pl.ot)) {
+                btree_set_ordered(pl.bs, pl.ot.tab, pl.ot.order, pl.ot.nlist);
+                pl.ordered = true;
+            }
+        }
         pl.scratch_keys = pl.bs.nscratch;
     }
     // + 16 bytes: the scratch starts at the array's own offset within 16 bytes
@@ -353,6 +392,18 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, wc, flags);
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
+        if (pl.ordered) {
+            if (pl.ot.nlist) {
+                int fper = 0;
+                TL_CUDA_TRY(
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fper, btree_fix_kernel<K>, kScatterThreads, 0));
+                const uint64_t fg = std::min<uint64_t>((pl.ot.nlist * 32 + kScatterThreads - 1) / kScatterThreads,
+                                                       (uint64_t)std::max(fper, 1) * smx);
+                btree_fix_kernel<K><<<(unsigned)fg, kScatterThreads, 0, st>>>(A, scr, pl.bs, pl.ot.list, pl.ot.nlist);
+                TL_CUDA_TRY(cudaGetLastError());
+            }
+            return TL_SUCCESS;
+        }
         BulkPlan bp;
         int rc = make_bulk_plan(pl.bs, A, scr, bp);
         if (rc) return rc;
@@ -389,8 +440,35 @@ static void keep_pool_memory() {
 
 int btree_plan_of(uint64_t n, uint64_t b) {
     PermutePlan pl;
-    if (make_plan(TL_LAYOUT_BTREE, n, b, 8, pl)) return -1;
+    if (make_plan(TL_LAYOUT_BTREE, n, b, 8, pl, ORDER_NEVER)) return -1;
     return pl.bs.plan;
+}
+
+int stream_blocks_per_sm(int layout, uint32_t key_bytes) {
+    const size_t smem = 32768 + 16;
+    int per_sm = 0;
+    cudaError_t e;
+    if (is_veb_layout(layout))
+        e = key_bytes == 8 ? cudaFuncSetAttribute(mveb_stream_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(mveb_stream_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else
+        e = key_bytes == 8 ? cudaFuncSetAttribute(btree_stream_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(btree_stream_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return -1;
+    if (is_veb_layout(layout))
+        e = key_bytes == 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mveb_stream_kernel<uint64_t>, kStreamThreads, smem)
+                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mveb_stream_kernel<uint32_t>, kStreamThreads, smem);
+    else
+        e = key_bytes == 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, btree_stream_kernel<uint64_t>, kStreamThreads, smem)
+                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, btree_stream_kernel<uint32_t>, kStreamThreads, smem);
+    return e == cudaSuccess ? per_sm : -1;
+}
+
+int permute_plan_of(int layout, uint64_t n, uint64_t b, uint32_t key_bytes) {
+    PermutePlan pl;
+    const int rc = make_plan(layout, n, b, key_bytes, pl);
+    if (rc) return -rc;
+    return is_veb_layout(layout) ? 3 : pl.bs.plan;
 }
 
 int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys) {
@@ -400,6 +478,14 @@ int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes,
     if (rc) return rc;
     if (is_veb_layout(layout)) {
         *keys = pl.mp.plan.total_slots;
+    } else if (pl.ordered) {
+        uint64_t c = 0;
+        for (uint64_t i = 0; i < pl.ot.nlist; ++i)
+            btree_fix_tile_host(pl.bs, pl.ot.list[i], [&](uint64_t, uint64_t len) {
+                c += len;
+                return true;
+            });
+        *keys = c;
     } else {
         *keys = 0;
         CopyRange r;
@@ -418,17 +504,39 @@ int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_byt
     return TL_SUCCESS;
 }
 
+int permute_workspace_bytes_fixed(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes) {
+    if (!bytes) return TL_ERROR_INVALID_VALUE;
+    PermutePlan pl;
+    int rc = make_plan(layout, n, b, key_bytes, pl, ORDER_NEVER);
+    if (rc) return rc;
+    *bytes = pl.bytes;
+    return TL_SUCCESS;
+}
+
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
-            uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms) {
+            uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms, bool allow_ordered) {
     if (n > 0 && !dev_A) return TL_ERROR_INVALID_VALUE;
     if (reinterpret_cast<uintptr_t>(dev_A) % (key_bytes ? key_bytes : 1)) return TL_ERROR_INVALID_VALUE;
     if (dev_ws && reinterpret_cast<uintptr_t>(dev_ws) % 256) return TL_ERROR_INVALID_VALUE;
     PermutePlan pl;
-    int rc = make_plan(layout, n, b, key_bytes, pl);
+    int rc = make_plan(layout, n, b, key_bytes, pl, allow_ordered ? ORDER_AUTO : ORDER_NEVER);
     if (rc) return rc;
     if (n <= 1) {
         if (ms) *ms = 0.f;
         return TL_SUCCESS;
+    }
+    // plan O needs its tile tables on the device and a scratch over every
+    // position; without either, the fixed-direction plan
+    if (pl.ordered) {
+        OrderTables dt;
+        if ((dev_ws && ws_bytes < pl.bytes) || !btree_order_device(pl.bs, st, dt)) {
+            rc = make_plan(layout, n, b, key_bytes, pl, ORDER_NEVER);
+            if (rc) return rc;
+        } else {
+            pl.ot = dt;
+            pl.bs.tab = dt.tab;
+            pl.bs.order = dt.order;
+        }
     }
     if (dev_ws && ws_bytes < pl.bytes) return TL_ERROR_WORKSPACE_TOO_SMALL;
     EventTimer timer(ms != nullptr || phase_ms != nullptr, st);
@@ -450,10 +558,13 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
     if (rc == TL_SUCCESS) {
         Ctrl *ctrl = reinterpret_cast<Ctrl *>(ws + pl.off_ctrl);
         rc = read_error_word(&ctrl->error, &err, st);
+        if (rc == TL_SUCCESS) record_wait_stats(ctrl, st);
     }
     if (owned) cudaFreeAsync(ws, st);
     if (rc == TL_SUCCESS) rc = sync_and_check(st);
-    if (rc == TL_SUCCESS && err) rc = TL_ERROR_TIMEOUT;
+    // a bounded wait expired, or (never expected) the ordered schedule found a
+    // scratch store without scratch and skipped it
+    if (rc == TL_SUCCESS && err) rc = (err & (1u << TL_ERROR_TIMEOUT)) ? TL_ERROR_TIMEOUT : TL_ERROR_UNSUPPORTED;
     if (rc == TL_SUCCESS && ms) *ms = timer.elapsed();
     if (rc == TL_SUCCESS && phase_ms) timer.elapsed_split(&phase_ms[0], &phase_ms[1]);
     return rc;
@@ -466,10 +577,22 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
 // by the tiles it waits for, a wait on a tile with a later ticket, and a final
 // position or scratch slot written other than exactly once.  Test hook only.
 static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *A,
-                              uint64_t *violations) {
+                              uint64_t *violations, int order_mode) {
     PermutePlan pl;
-    int rc = make_plan(layout, n, b, key_bytes, pl);
+    int rc = make_plan(layout, n, b, key_bytes, pl, ORDER_NEVER);
     if (rc) return rc;
+    OrderVectors ov;  // computed here, not taken from the library's cache
+    if (order_mode != ORDER_NEVER && !is_veb_layout(layout)) {
+        btree_compute_order(pl.bs, ov);
+        const OrderTables ot = ov.tables();
+        rc = make_plan(layout, n, b, key_bytes, pl, order_mode, &ot);
+        if (rc) return rc;
+    }
+    // tile kk's ticket precedes (or is) tile k's
+    auto earlier = [&](uint64_t kk, uint64_t k) {
+        if (pl.ordered) return btree_o_rank(pl.bs, kk) <= btree_o_rank(pl.bs, k);
+        return pl.bs.plan == PLAN_R ? kk >= k : kk <= k;
+    };
     uint64_t viol = 0;
     if (n > 1) {
         std::vector<uint64_t> scr(pl.scratch_keys, 0), tile(pl.tile_keys + 1);
@@ -492,8 +615,9 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                                  : btree_tile_wait(pl.bs, p0, p1, k_lo, k_hi);
             if (wait)
                 for (uint64_t kk = k_lo; kk <= k_hi; ++kk) {
-                    const bool earlier = (mv || pl.bs.plan == PLAN_R) ? kk > k : kk < k;
-                    if (!earlier || !readk[kk]) ++viol;
+                    if (pl.ordered && !btree_o_direct(pl.bs, k, kk)) continue;  // not waited for
+                    const bool ok = mv ? kk > k : pl.ordered ? earlier(kk, k) : pl.bs.plan == PLAN_R ? kk > k : kk < k;
+                    if (!ok || !readk[kk]) ++viol;
                 }
             auto W = [&](uint64_t d, uint64_t v) {
                 if (d >= n) { ++viol; return; }
@@ -521,13 +645,20 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                 uint32_t cum[kMaxTopRuns + 1], wlo[kMaxTopRuns + 1], whi[kMaxTopRuns + 1], nw = 0;
                 cum[0] = 0;
                 for (uint32_t sl = 0; sl < nr; ++sl) {
-                    runs[sl] = btree_group_run(S, sl < kMaxTopLevels ? G0 : G1, sl % kMaxTopLevels);
+                    runs[sl] = btree_group_run(S, sl < kMaxTopLevels ? G0 : G1, sl % kMaxTopLevels, k);
                     cum[sl + 1] = cum[sl] + runs[sl].cnt;
                 }
                 uint64_t a, bq;
+                std::vector<uint64_t> wl;  // plan O: the tiles the bulk stores wait for
                 if (btree_tile_wait(S, p0, p1, a, bq)) {
-                    wlo[nw] = (uint32_t)a;
-                    whi[nw++] = (uint32_t)bq;
+                    if (pl.ordered) {
+                        for (uint64_t kk = a; kk <= bq; ++kk) {
+                            if (btree_o_direct(S, k, kk)) wl.push_back(kk);
+                        }
+                    } else {
+                        wlo[nw] = (uint32_t)a;
+                        whi[nw++] = (uint32_t)bq;
+                    }
                 }
                 for (uint32_t sl = 0; sl < nr; ++sl)
                     if (runs[sl].cnt && btree_run_wait(S, runs[sl], a, bq)) {
@@ -535,14 +666,16 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                         whi[nw++] = (uint32_t)bq;
                     }
                 for (uint32_t w = 0; w < nw; ++w)
-                    for (uint64_t kk = wlo[w]; kk <= whi[w]; ++kk) {
-                        const bool earlier = pl.bs.plan == PLAN_R ? kk >= k : kk <= k;
-                        if (!earlier || !readk[kk]) ++viol;
-                    }
+                    for (uint64_t kk = wlo[w]; kk <= whi[w]; ++kk)
+                        if (!earlier(kk, k) || !readk[kk]) ++viol;
+                for (uint64_t kk : wl)
+                    if (!earlier(kk, k) || !readk[kk]) ++viol;
                 auto covered_tile = [&](uint64_t kd) {
                     if (kd == k) return true;
                     for (uint32_t w = 0; w < nw; ++w)
                         if (kd >= wlo[w] && kd <= whi[w]) return true;
+                    for (uint64_t kk : wl)
+                        if (kd == kk) return true;
                     return false;
                 };
                 auto WD = [&](uint64_t d, uint64_t v) {  // direct store, checked against the wait list
@@ -562,9 +695,12 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                         if (btree_place(S, x, idx)) WD(idx, tile[o]); else SC(idx, tile[o]);
                     } else {
                         if (RG.kind == 2 || !btree_regime_bulk(S, RG, o, idx)) continue;
+                        const bool hi = RG.kind == 3 && idx >= RG.dsplit;
+                        const bool to_A = hi ? RG.hi_A : RG.to_A;
+                        if (RG.kind == 3 && !to_A) idx += (uint64_t)(hi ? RG.shi : RG.slo);
                         const bool direct = btree_place(S, x, ref);  // fast path == reference form
-                        if (direct != RG.to_A || ref != idx) ++viol;
-                        if (RG.to_A) WD(idx, tile[o]); else SC(idx, tile[o]);
+                        if (direct != to_A || ref != idx) ++viol;
+                        if (to_A) WD(idx, tile[o]); else SC(idx, tile[o]);
                     }
                     covered[o] = 1;
                 }
@@ -575,10 +711,13 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                         const uint64_t off = btree_top_item_off(S, runs[r], e);
                         if (off >= cnt || covered[off]) { ++viol; continue; }
                         const uint64_t p = runs[r].dest0 + e;
+                        const bool kdirect = btree_run_direct(S, runs[r], e);
+                        const uint64_t kidx =  // the kernel's store index
+                            kdirect || !pl.ordered ? p : p + (uint64_t)(e < runs[r].nlo ? runs[r].slo : runs[r].shi);
                         uint64_t ref;
                         const bool direct = btree_place(S, p0 + off, ref);
-                        if (direct != btree_run_direct(S, runs[r], e) || ref != p) ++viol;
-                        if (direct) WD(p, tile[off]); else SC(p, tile[off]);
+                        if (direct != kdirect || ref != kidx) ++viol;
+                        if (direct) WD(kidx, tile[off]); else SC(kidx, tile[off]);
                         covered[off] = 1;
                     }
                 }
@@ -606,8 +745,28 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
             }
         }
         if (!mv) {
-            for (uint64_t c = 0; c < pl.bs.nscratch; ++c)
-                if (slot_writes[c] != (btree_slot_used(pl.bs, c) ? 1u : 0u)) ++viol;
+            if (pl.ordered) {  // the fix pass over the listed tiles; every slot it reads written once
+                std::vector<uint8_t> read_slot(pl.bs.nscratch, 0);
+                for (uint64_t i = 0; i < pl.ot.nlist; ++i) {
+                    const uint64_t u = pl.ot.list[i];
+                    const int64_t so = btree_o_soff(pl.bs, u);
+                    btree_fix_tile_host(pl.bs, u, [&](uint64_t pa, uint64_t len) {
+                        for (uint64_t d = pa; d < pa + len; ++d) {
+                            const uint64_t sl = d + (uint64_t)so;
+                            if (d >= n || sl >= pl.bs.nscratch || slot_writes[sl] != 1) { ++viol; continue; }
+                            A[d] = scr[sl];
+                            ++pos_writes[d];
+                            read_slot[sl] = 1;
+                        }
+                        return true;
+                    });
+                }
+                for (uint64_t c = 0; c < pl.bs.nscratch; ++c)
+                    if (slot_writes[c] != read_slot[c]) ++viol;
+            } else {
+                for (uint64_t c = 0; c < pl.bs.nscratch; ++c)
+                    if (slot_writes[c] != (btree_slot_used(pl.bs, c) ? 1u : 0u)) ++viol;
+            }
             for (int j = 0; j < btree_copy_range_count(pl.bs); ++j) {
                 CopyRange cr;
                 if (!btree_copy_range(pl.bs, j, cr)) continue;
@@ -635,17 +794,19 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
     return TL_SUCCESS;
 }
 
-// Replays the plans of both key widths (their tile sizes and scratch alignment
-// differ); the results must agree.
+// Replays the ordered schedule (plan O wherever it applies) at both key widths
+// (their tile sizes and scratch alignment differ) and the fixed-direction
+// schedule; the results must agree.
 int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations) {
-    std::vector<uint64_t> A4(A, A + n);
-    uint64_t v8 = 0, v4 = 0;
-    int rc = emulate_permute_kb(layout, n, b, 8, A, &v8);
-    if (!rc) rc = emulate_permute_kb(layout, n, b, 4, A4.data(), &v4);
+    std::vector<uint64_t> A4(A, A + n), Af(A, A + n);
+    uint64_t v8 = 0, v4 = 0, vf = 0;
+    int rc = emulate_permute_kb(layout, n, b, 8, A, &v8, ORDER_ALWAYS);
+    if (!rc) rc = emulate_permute_kb(layout, n, b, 4, A4.data(), &v4, ORDER_ALWAYS);
+    if (!rc) rc = emulate_permute_kb(layout, n, b, 8, Af.data(), &vf, ORDER_NEVER);
     if (rc) return rc;
     uint64_t diff = 0;
-    for (uint64_t x = 0; x < n; ++x) diff += A[x] != A4[x];
-    if (violations) *violations = v8 + v4 + diff;
+    for (uint64_t x = 0; x < n; ++x) diff += (A[x] != A4[x]) + (A[x] != Af[x]);
+    if (violations) *violations = v8 + v4 + vf + diff;
     return TL_SUCCESS;
 }
 

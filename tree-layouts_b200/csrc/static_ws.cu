@@ -61,12 +61,14 @@ static int static_workspace(void **ptr) {
 extern "C" int tl_permute_static_ws(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                                     void *stream) {
     uint64_t need = 0;
-    int rc = tl::permute_workspace_bytes(layout, n, b, key_bytes, &need);
+    int rc = tl::permute_workspace_bytes_fixed(layout, n, b, key_bytes, &need);
     if (rc) return rc;
     if (need > tl::kStaticWorkspaceBytes) return TL_ERROR_UNSUPPORTED;
     void *ws = nullptr;
     rc = tl::static_workspace(&ws);
     if (rc) return rc;
+    // the fixed-direction schedules only: the ordered one keeps device tables
+    // that the library would have to allocate
     return tl::permute(layout, dev_A, n, b, key_bytes, ws, tl::kStaticWorkspaceBytes,
-                       reinterpret_cast<cudaStream_t>(stream), nullptr);
+                       reinterpret_cast<cudaStream_t>(stream), nullptr, nullptr, false);
 }

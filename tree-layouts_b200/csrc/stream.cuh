@@ -21,7 +21,10 @@ namespace tl {
 struct Ctrl {
     unsigned long long ticket;
     unsigned int error;
-    unsigned int pad[13];
+    unsigned int pad0;
+    unsigned long long stalled_waits;  // waits whose flag was not set at the first look
+    unsigned long long stall_polls;    // polls those waits took
+    unsigned int pad[8];
 };
 
 // Wait parameters, passed to the kernels by value.
@@ -47,7 +50,13 @@ __device__ __forceinline__ bool wait_flag(const unsigned int *flag, unsigned int
     unsigned int limit = wc.spin_limit;
     unsigned int ns = 32;
     for (unsigned int it = 0; it <= limit; ++it) {
-        if (ld_acquire(flag) == want) return true;
+        if (ld_acquire(flag) == want) {
+            if (it) {
+                atomicAdd(&ctrl->stalled_waits, 1ull);
+                atomicAdd(&ctrl->stall_polls, (unsigned long long)it);
+            }
+            return true;
+        }
         __nanosleep(ns);
         if (ns < 256) ns <<= 1;
     }
@@ -96,8 +105,18 @@ __device__ __forceinline__ unsigned long long ticket_advance(const TicketPipe &t
 // address.  Returns base when the copy has landed.  The 16-byte-aligned interior
 // goes through cp.async (global -> shared without registers), so every thread
 // has all of its copies in flight at once; the ragged ends use plain loads.
+// The base of load_tile for a tile starting at p0.
 template <typename K>
-__device__ __forceinline__ uint64_t load_tile(const K *__restrict__ src, uint64_t p0, uint64_t p1, K *sm) {
+__device__ __forceinline__ uint64_t tile_base(const K *src, uint64_t p0) {
+    return p0 - (reinterpret_cast<uintptr_t>(src + p0) & 15) / sizeof(K);
+}
+
+// load_tile in two halves: issue returns base with the interior's copies still
+// in flight; load_tile_wait waits for them.  Threads tid of nt (default: the
+// whole block) share the copies.
+template <typename K>
+__device__ __forceinline__ uint64_t load_tile_issue(const K *__restrict__ src, uint64_t p0, uint64_t p1, K *sm,
+                                                    uint32_t tid = threadIdx.x, uint32_t nt = blockDim.x) {
     constexpr uint32_t V = 16 / sizeof(K);
     uintptr_t addr0 = reinterpret_cast<uintptr_t>(src + p0);
     uint64_t head = (addr0 & 15) / sizeof(K);  // elements before the 16-byte boundary
@@ -106,15 +125,23 @@ __device__ __forceinline__ uint64_t load_tile(const K *__restrict__ src, uint64_
     if (a0 > p1) a0 = p1;
     uint64_t nvec = (p1 - a0) / V;
     uint64_t a1 = a0 + nvec * V;
-    for (uint64_t x = p0 + threadIdx.x; x < a0; x += blockDim.x) sm[x - base] = src[x];
+    for (uint64_t x = p0 + tid; x < a0; x += nt) sm[x - base] = src[x];
     const char *gsrc = reinterpret_cast<const char *>(src + a0);
     const uint32_t sdst = (uint32_t)__cvta_generic_to_shared(sm + (a0 - base));
-    for (uint64_t v = threadIdx.x; v < nvec; v += blockDim.x)
+    for (uint64_t v = tid; v < nvec; v += nt)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst + (uint32_t)(v * 16)),
                      "l"(gsrc + v * 16)
                      : "memory");
-    for (uint64_t x = a1 + threadIdx.x; x < p1; x += blockDim.x) sm[x - base] = src[x];
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    for (uint64_t x = a1 + tid; x < p1; x += nt) sm[x - base] = src[x];
+    return base;
+}
+
+__device__ __forceinline__ void load_tile_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <typename K>
+__device__ __forceinline__ uint64_t load_tile(const K *__restrict__ src, uint64_t p0, uint64_t p1, K *sm) {
+    const uint64_t base = load_tile_issue(src, p0, p1, sm);
+    load_tile_wait();
     return base;
 }
 
