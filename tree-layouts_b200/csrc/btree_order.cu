@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "btree_order.h"
+#include "bulk.cuh"
 #include "internal.h"
 
 namespace tl {
@@ -88,8 +89,8 @@ static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, boo
         v.tab[u].x = (uint32_t)t;
     }
     S.tab = v.tab.data();
-    v.list.clear();
-    uint64_t keys = 0;
+    std::vector<uint8_t> full(N, 0);
+    uint64_t keys = 0, slots = 0;
     for (uint64_t u = 0; u < N; ++u) {
         uint64_t c = 0;
         btree_fix_tile_host(S, u, [&](uint64_t, uint64_t len) {
@@ -98,9 +99,33 @@ static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, boo
         });
         if (!c) continue;
         keys += c;
-        v.tab[u].y = (uint32_t)v.list.size();
-        v.list.push_back((uint32_t)u);
+        v.tab[u].y = (uint32_t)slots++;
+        full[u] = c == std::min<uint64_t>(S.tile_keys, S.g.n - (u << S.tile_shift));
     }
+    v.scratch_tiles = slots;
+    // runs of consecutive full tiles (their slots are consecutive too): the
+    // longest go to the bulk-copy engine
+    std::vector<uint4> runs;
+    for (uint64_t u = 0; u < N;) {
+        if (!full[u]) {
+            ++u;
+            continue;
+        }
+        uint64_t w = u;
+        while (w < N && full[w]) ++w;
+        runs.push_back(make_uint4((uint32_t)u, (uint32_t)w, v.tab[u].y, 0));
+        u = w;
+    }
+    std::stable_sort(runs.begin(), runs.end(), [](uint4 a, uint4 b) { return a.y - a.x > b.y - b.x; });
+    if (runs.size() > (size_t)kMaxBulkRanges) runs.resize(kMaxBulkRanges);
+    std::sort(runs.begin(), runs.end(), [](uint4 a, uint4 b) { return a.x < b.x; });
+    v.ranges = runs;
+    std::vector<uint8_t> bulk(N, 0);
+    for (const uint4 &r : runs)
+        for (uint32_t u = r.x; u < r.y; ++u) bulk[u] = 1;
+    v.list.clear();
+    for (uint64_t u = 0; u < N; ++u)
+        if (v.tab[u].y != kNoSlot && !bulk[u]) v.list.push_back((uint32_t)u);
     return keys;
 }
 
@@ -203,6 +228,9 @@ bool btree_order_device(const BtreeStream &S, cudaStream_t st, OrderTables &t) {
     t.order = reinterpret_cast<const uint32_t *>(p + N * sizeof(uint2));
     t.list = t.order + N;
     t.nlist = L;
+    t.ranges = e->v.ranges.data();
+    t.nranges = e->v.ranges.size();
+    t.scratch_tiles = e->v.scratch_tiles;
     return true;
 }
 

@@ -7,24 +7,36 @@
 
 namespace tl {
 
-// The tables of plan O for one geometry (host or device pointers).
+// The tables of plan O for one geometry (tab, order and list: host or device
+// pointers; ranges: host).  The tiles that receive scratch keys own a tile of
+// scratch each, in ascending order; runs of consecutive tiles whose every key
+// goes through scratch are copied back as ranges by the bulk-copy engine (at
+// most kMaxBulkRanges of them, the longest), the other tiles by the fix pass.
 struct OrderTables {
     const uint2 *tab = nullptr;       // per tile {ticket, scratch slot or kNoSlot}
     const uint32_t *order = nullptr;  // tile of each ticket
-    const uint32_t *list = nullptr;   // the tiles that receive scratch keys, ascending (slot order)
+    const uint32_t *list = nullptr;   // tiles for the fix pass, ascending
     uint64_t nlist = 0;
+    const uint4 *ranges = nullptr;    // tiles [x, y) from scratch slot z on, for the bulk-copy engine
+    uint64_t nranges = 0;
+    uint64_t scratch_tiles = 0;
 };
 
 // Host vectors behind an OrderTables.
 struct OrderVectors {
     std::vector<uint2> tab;
+    std::vector<uint4> ranges;
     std::vector<uint32_t> order, list;
+    uint64_t scratch_tiles = 0;
     OrderTables tables() const {
         OrderTables t;
         t.tab = tab.data();
         t.order = order.data();
         t.list = list.data();
         t.nlist = list.size();
+        t.ranges = ranges.data();
+        t.nranges = ranges.size();
+        t.scratch_tiles = scratch_tiles;
         return t;
     }
 };

@@ -72,44 +72,61 @@ btree_copy_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_con
     bulk_copy_plan(A, scr, P, stage, bars, ctrl);
 }
 
-// Second pass of a plan-O B-tree permutation: one warp per destination tile
-// that receives scratch keys (list[0, nlist)).
+// Second pass of a plan-O B-tree permutation for the destination tiles
+// list[0, nlist) (those not copied as whole-tile ranges): a block per tile.
 template <typename K>
 __global__ void __launch_bounds__(kScatterThreads)
 btree_fix_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_constant__ BtreeStream S,
                  const uint32_t *__restrict__ list, uint64_t nlist) {
-    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = w; i < nlist; i += nw) btree_fix_tile_warp(S, A, scr, (uint64_t)__ldg(list + i));
+    for (uint64_t i = blockIdx.x; i < nlist; i += gridDim.x) btree_fix_tile_block(S, A, scr, (uint64_t)__ldg(list + i));
 }
 
-// The copy ranges split for the bulk engine: each range's 16-byte-aligned
-// interior in kBulkChunk pieces, its ragged keys apart.  The scratch shares A's
-// offset within 16 bytes at both range bases, so the interiors line up.
+// One copy range for the bulk engine: its 16-byte-aligned interior in
+// kBulkChunk pieces, its ragged keys apart.  The scratch shares A's offset
+// within 16 bytes at both range bases, so the interiors line up.
 template <typename K>
-static int make_bulk_plan(const BtreeStream &S, const K *A, const K *scr, BulkPlan &P) {
+static int add_bulk_range(const K *A, const K *scr, const CopyRange &r, BulkPlan &P) {
+    if (P.nr == kMaxBulkRanges) return TL_ERROR_UNSUPPORTED;
+    const uintptr_t da = reinterpret_cast<uintptr_t>(A + r.dst), sa = reinterpret_cast<uintptr_t>(scr + r.src);
+    if ((da ^ sa) & 15) return TL_ERROR_INVALID_VALUE;
+    BulkRange R{};
+    R.key_dst = r.dst;
+    R.key_src = r.src;
+    R.len = r.len;
+    const uint64_t head = std::min<uint64_t>(((16 - (da & 15)) & 15) / sizeof(K), r.len);
+    const uint64_t body = ((r.len - head) * sizeof(K)) & ~15ull;
+    R.head = (uint32_t)head;
+    R.tail = (uint32_t)(r.len - head - body / sizeof(K));
+    R.dst = (r.dst + head) * sizeof(K);
+    R.src = (r.src + head) * sizeof(K);
+    R.bytes = body;
+    R.chunk0 = P.nchunks;
+    P.nchunks += (body + kBulkChunk - 1) / kBulkChunk;
+    P.r[P.nr++] = R;
+    return TL_SUCCESS;
+}
+
+// The copy ranges of a plan: per level (plans R, L), or the runs of whole
+// scratch tiles (plan O: tiles [x, y) from scratch slot z on).
+template <typename K>
+static int make_bulk_plan(const BtreeStream &S, const OrderTables &ot, const K *A, const K *scr, BulkPlan &P) {
     P.nr = 0;
     P.nchunks = 0;
+    if (S.plan == PLAN_O) {
+        for (uint64_t i = 0; i < ot.nranges; ++i) {
+            const uint64_t u0 = ot.ranges[i].x, u1 = ot.ranges[i].y;
+            const uint64_t d0 = u0 << S.tile_shift, d1 = std::min<uint64_t>(u1 << S.tile_shift, S.g.n);
+            const uint64_t s0 = (uint64_t)ot.ranges[i].z << S.tile_shift;  // host data: S.tab may be device memory
+            const int rc = add_bulk_range(A, scr, CopyRange{d0, s0, d1 - d0}, P);
+            if (rc) return rc;
+        }
+        return TL_SUCCESS;
+    }
     for (int j = 0; j < btree_copy_range_count(S); ++j) {
         CopyRange r;
         if (!btree_copy_range(S, j, r)) continue;
-        if (P.nr == kMaxBulkRanges) return TL_ERROR_UNSUPPORTED;
-        const uintptr_t da = reinterpret_cast<uintptr_t>(A + r.dst), sa = reinterpret_cast<uintptr_t>(scr + r.src);
-        if ((da ^ sa) & 15) return TL_ERROR_INVALID_VALUE;
-        BulkRange R{};
-        R.key_dst = r.dst;
-        R.key_src = r.src;
-        R.len = r.len;
-        const uint64_t head = std::min<uint64_t>(((16 - (da & 15)) & 15) / sizeof(K), r.len);
-        const uint64_t body = ((r.len - head) * sizeof(K)) & ~15ull;
-        R.head = (uint32_t)head;
-        R.tail = (uint32_t)(r.len - head - body / sizeof(K));
-        R.dst = (r.dst + head) * sizeof(K);
-        R.src = (r.src + head) * sizeof(K);
-        R.bytes = body;
-        R.chunk0 = P.nchunks;
-        P.nchunks += (body + kBulkChunk - 1) / kBulkChunk;
-        P.r[P.nr++] = R;
+        const int rc = add_bulk_range(A, scr, r, P);
+        if (rc) return rc;
     }
     return TL_SUCCESS;
 }
@@ -326,7 +343,7 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
              (order_mode == ORDER_AUTO && pl.ntiles >= kOrderMinTiles && !g_fixed_only))) {
             if (tables) pl.ot = *tables;
             if (tables || btree_order_host(pl.bs, pl.ot)) {
-                btree_set_ordered(pl.bs, pl.ot.tab, pl.ot.order, pl.ot.nlist);
+                btree_set_ordered(pl.bs, pl.ot.tab, pl.ot.order, pl.ot.scratch_tiles);
                 pl.ordered = true;
             }
         }
@@ -392,20 +409,15 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, wc, flags);
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
-        if (pl.ordered) {
-            if (pl.ot.nlist) {
-                int fper = 0;
-                TL_CUDA_TRY(
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fper, btree_fix_kernel<K>, kScatterThreads, 0));
-                const uint64_t fg = std::min<uint64_t>((pl.ot.nlist * 32 + kScatterThreads - 1) / kScatterThreads,
-                                                       (uint64_t)std::max(fper, 1) * smx);
-                btree_fix_kernel<K><<<(unsigned)fg, kScatterThreads, 0, st>>>(A, scr, pl.bs, pl.ot.list, pl.ot.nlist);
-                TL_CUDA_TRY(cudaGetLastError());
-            }
-            return TL_SUCCESS;
+        if (pl.ordered && pl.ot.nlist) {
+            int fper = 0;
+            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fper, btree_fix_kernel<K>, kScatterThreads, 0));
+            const uint64_t fg = std::min<uint64_t>(pl.ot.nlist, (uint64_t)std::max(fper, 1) * smx);
+            btree_fix_kernel<K><<<(unsigned)fg, kScatterThreads, 0, st>>>(A, scr, pl.bs, pl.ot.list, pl.ot.nlist);
+            TL_CUDA_TRY(cudaGetLastError());
         }
         BulkPlan bp;
-        int rc = make_bulk_plan(pl.bs, A, scr, bp);
+        int rc = make_bulk_plan(pl.bs, pl.ot, A, scr, bp);
         if (rc) return rc;
         if (bp.nr) {
             // one warp per CTA, as many CTAs per SM as the stages' shared memory allows
@@ -480,6 +492,9 @@ int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes,
         *keys = pl.mp.plan.total_slots;
     } else if (pl.ordered) {
         uint64_t c = 0;
+        for (uint64_t i = 0; i < pl.ot.nranges; ++i)
+            c += std::min<uint64_t>((uint64_t)pl.ot.ranges[i].y << pl.bs.tile_shift, n) -
+                 ((uint64_t)pl.ot.ranges[i].x << pl.bs.tile_shift);
         for (uint64_t i = 0; i < pl.ot.nlist; ++i)
             btree_fix_tile_host(pl.bs, pl.ot.list[i], [&](uint64_t, uint64_t len) {
                 c += len;
@@ -745,15 +760,29 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
             }
         }
         if (!mv) {
-            if (pl.ordered) {  // the fix pass over the listed tiles; every slot it reads written once
+            if (pl.ordered) {  // the bulk ranges and the fix pass; every slot they read written once
                 std::vector<uint8_t> read_slot(pl.bs.nscratch, 0);
+                for (uint64_t i = 0; i < pl.ot.nranges; ++i) {
+                    const uint64_t u0 = pl.ot.ranges[i].x;
+                    const uint64_t d0 = u0 * pl.tile_keys, d1 = std::min<uint64_t>(pl.ot.ranges[i].y * pl.tile_keys, n);
+                    for (uint64_t d = d0; d < d1; ++d) {
+                        const uint64_t sl = d + (uint64_t)btree_o_soff(pl.bs, d / pl.tile_keys);
+                        if (sl >= pl.bs.nscratch || slot_writes[sl] != 1 || read_slot[sl]) { ++viol; continue; }
+                        A[d] = scr[sl];
+                        ++pos_writes[d];
+                        read_slot[sl] = 1;
+                    }
+                }
                 for (uint64_t i = 0; i < pl.ot.nlist; ++i) {
                     const uint64_t u = pl.ot.list[i];
                     const int64_t so = btree_o_soff(pl.bs, u);
                     btree_fix_tile_host(pl.bs, u, [&](uint64_t pa, uint64_t len) {
                         for (uint64_t d = pa; d < pa + len; ++d) {
                             const uint64_t sl = d + (uint64_t)so;
-                            if (d >= n || sl >= pl.bs.nscratch || slot_writes[sl] != 1) { ++viol; continue; }
+                            if (d >= n || sl >= pl.bs.nscratch || slot_writes[sl] != 1 || read_slot[sl]) {
+                                ++viol;
+                                continue;
+                            }
                             A[d] = scr[sl];
                             ++pos_writes[d];
                             read_slot[sl] = 1;
