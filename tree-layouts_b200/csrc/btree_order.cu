@@ -123,9 +123,25 @@ static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, boo
     std::vector<uint8_t> bulk(N, 0);
     for (const uint4 &r : runs)
         for (uint32_t u = r.x; u < r.y; ++u) bulk[u] = 1;
-    v.list.clear();
-    for (uint64_t u = 0; u < N; ++u)
-        if (v.tab[u].y != kNoSlot && !bulk[u]) v.list.push_back((uint32_t)u);
+    // the fix pass's copies: the scratch runs of the other tiles, adjacent ones merged
+    v.segs.clear();
+    for (uint64_t u = 0; u < N; ++u) {
+        if (v.tab[u].y == kNoSlot || bulk[u]) continue;
+        const int64_t so = btree_o_soff(S, u);
+        btree_fix_tile_host(S, u, [&](uint64_t pa, uint64_t len) {
+            const uint64_t src = pa + (uint64_t)so;
+            if (!v.segs.empty()) {
+                FixSeg &l = v.segs.back();
+                const uint64_t ld = l.dst_len & kSegDstMask, ll = l.dst_len >> 48;
+                if (ld + ll == pa && l.src + ll == src && ll + len <= kFixSegMax) {
+                    l.dst_len = ld | ((ll + len) << 48);
+                    return true;
+                }
+            }
+            v.segs.push_back(FixSeg{pa | (len << 48), src});
+            return true;
+        });
+    }
     return keys;
 }
 
@@ -170,7 +186,7 @@ namespace {
 struct OrderEntry {
     uint64_t n, b, tile_keys;
     OrderVectors v;
-    void *dev[kMaxOrderDevices] = {};  // tab, then order and list
+    void *dev[kMaxOrderDevices] = {};  // segs, then tab and order
 };
 std::mutex g_order_mu;
 std::vector<std::unique_ptr<OrderEntry>> g_orders;
@@ -203,20 +219,20 @@ bool btree_order_device(const BtreeStream &S, cudaStream_t st, OrderTables &t) {
     std::lock_guard<std::mutex> lk(g_order_mu);
     OrderEntry *e = order_entry_locked(S);
     if (!e) return false;
-    const uint64_t N = S.ntiles, L = e->v.list.size();
+    const uint64_t N = S.ntiles, L = e->v.segs.size();
     if (!e->dev[dev]) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
         char *p = nullptr;
-        const size_t o1 = N * sizeof(uint2), o2 = o1 + N * sizeof(uint32_t);
-        if (cudaMalloc(reinterpret_cast<void **>(&p), o2 + L * sizeof(uint32_t)) != cudaSuccess) {
+        const size_t o1 = L * sizeof(FixSeg), o2 = o1 + N * sizeof(uint2);
+        if (cudaMalloc(reinterpret_cast<void **>(&p), o2 + N * sizeof(uint32_t)) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
         // synchronous copies from pageable memory: done before the tables are used
-        if (cudaMemcpy(p, e->v.tab.data(), o1, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(p + o1, e->v.order.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
-            (L && cudaMemcpy(p + o2, e->v.list.data(), L * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)) {
+        if ((L && cudaMemcpy(p, e->v.segs.data(), o1, cudaMemcpyHostToDevice) != cudaSuccess) ||
+            cudaMemcpy(p + o1, e->v.tab.data(), N * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(p + o2, e->v.order.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
             cudaGetLastError();
             cudaFree(p);
             return false;
@@ -224,10 +240,10 @@ bool btree_order_device(const BtreeStream &S, cudaStream_t st, OrderTables &t) {
         e->dev[dev] = p;
     }
     const char *p = static_cast<const char *>(e->dev[dev]);
-    t.tab = reinterpret_cast<const uint2 *>(p);
-    t.order = reinterpret_cast<const uint32_t *>(p + N * sizeof(uint2));
-    t.list = t.order + N;
-    t.nlist = L;
+    t.segs = reinterpret_cast<const FixSeg *>(p);
+    t.nsegs = L;
+    t.tab = reinterpret_cast<const uint2 *>(p + L * sizeof(FixSeg));
+    t.order = reinterpret_cast<const uint32_t *>(p + L * sizeof(FixSeg) + N * sizeof(uint2));
     t.ranges = e->v.ranges.data();
     t.nranges = e->v.ranges.size();
     t.scratch_tiles = e->v.scratch_tiles;

@@ -7,16 +7,25 @@
 
 namespace tl {
 
-// The tables of plan O for one geometry (tab, order and list: host or device
+// A copy of the fix pass: len keys from scratch index src on to position dst
+// on; dst in the low 48 bits of dst_len, len (at most kFixSegMax) in the high 16.
+struct FixSeg {
+    uint64_t dst_len, src;
+};
+constexpr uint64_t kFixSegMax = 8192;
+constexpr uint64_t kSegDstMask = (1ull << 48) - 1;
+
+// The tables of plan O for one geometry (tab, order and segs: host or device
 // pointers; ranges: host).  The tiles that receive scratch keys own a tile of
 // scratch each, in ascending order; runs of consecutive tiles whose every key
 // goes through scratch are copied back as ranges by the bulk-copy engine (at
-// most kMaxBulkRanges of them, the longest), the other tiles by the fix pass.
+// most kMaxBulkRanges of them, the longest), the scratch keys of the other
+// tiles by the fix pass, as the host-listed copies segs.
 struct OrderTables {
     const uint2 *tab = nullptr;       // per tile {ticket, scratch slot or kNoSlot}
     const uint32_t *order = nullptr;  // tile of each ticket
-    const uint32_t *list = nullptr;   // tiles for the fix pass, ascending
-    uint64_t nlist = 0;
+    const FixSeg *segs = nullptr;     // the fix pass's copies
+    uint64_t nsegs = 0;
     const uint4 *ranges = nullptr;    // tiles [x, y) from scratch slot z on, for the bulk-copy engine
     uint64_t nranges = 0;
     uint64_t scratch_tiles = 0;
@@ -26,14 +35,15 @@ struct OrderTables {
 struct OrderVectors {
     std::vector<uint2> tab;
     std::vector<uint4> ranges;
-    std::vector<uint32_t> order, list;
+    std::vector<uint32_t> order;
+    std::vector<FixSeg> segs;
     uint64_t scratch_tiles = 0;
     OrderTables tables() const {
         OrderTables t;
         t.tab = tab.data();
         t.order = order.data();
-        t.list = list.data();
-        t.nlist = list.size();
+        t.segs = segs.data();
+        t.nsegs = segs.size();
         t.ranges = ranges.data();
         t.nranges = ranges.size();
         t.scratch_tiles = scratch_tiles;

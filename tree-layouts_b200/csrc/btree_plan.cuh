@@ -40,11 +40,12 @@ constexpr int kMaxTopRuns = 2 * kMaxTopLevels;  // a tile holds at most two grou
 // that can receive such keys own scratch (a tile's worth each, in the order of
 // the host's list of them), so soff(u) = (slot[u] - u) * tile_keys with slot[u]
 // u's index in that list.  rank and slot share one 8-byte entry per tile
-// (tab[u]), so a tile's decision and its scratch offset are one load.  The order puts each tile before the tile that feeds it most keys,
-// following those edges in chains, so that far fewer keys go through scratch
-// than under either fixed direction.  Its second pass copies runs of whole
-// scratch tiles with the bulk-copy engine and walks the other listed tiles
-// (btree_fix_tile_block).
+// (tab[u]), so a tile's decision and its scratch offset are one load.  The
+// order puts each tile before the tile that feeds it most keys, following those
+// edges in chains, so that far fewer keys go through scratch than under either
+// fixed direction.  Its second pass copies runs of whole scratch tiles with the
+// bulk-copy engine and the other scratch keys as host-listed segments
+// (btree_fix_kernel).
 enum BtreePlan { PLAN_R = 0, PLAN_L = 1, PLAN_O = 2 };
 
 struct BtreeStream {
@@ -845,13 +846,9 @@ TL_HD uint64_t btree_src_rank_at(const BtreeStream &S, uint32_t lv, uint64_t p) 
 template <class Visit>
 __host__ void btree_fix_tile_host(const BtreeStream &S, uint64_t u, Visit &&visit);
 
-// Device form, one block per tile (the tiles whose scratch keys are not part of
-// a whole-tile range).  A piece with few source tiles (at most kFixDense) has
-// long runs: when all of them went through scratch the block copies the piece
-// as one range, else each warp copies source runs with consecutive lanes on
-// consecutive keys.  A piece whose keys come from more tiles than that (a level
-// high in the tree, whose consecutive positions draw on distant tiles) is
-// walked position by position.
+// The device side of the fix pass copies host-listed segments (each made of
+// these runs) with warp_copy_keys.  Host enumeration: a piece with few source
+// tiles (below kFixDense) run by run, any other position by position.
 constexpr int kFixUnr = 8;
 constexpr uint64_t kFixDense = 64;
 
@@ -872,70 +869,6 @@ __device__ __forceinline__ void warp_copy_keys(K *__restrict__ dst, const K *__r
             const uint32_t x = q + r * 32 + lane;
             if (x < hi) dst[x] = v[r];
         }
-    }
-}
-
-template <typename K>
-__device__ __forceinline__ void btree_fix_tile_block(const BtreeStream &S, K *__restrict__ A,
-                                                     const K *__restrict__ scr, uint64_t u) {
-    const uint32_t tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, nwarps = nt >> 5;
-    const uint64_t P0 = u << S.tile_shift, P1 = P0 + S.tile_keys < S.g.n ? P0 + S.tile_keys : S.g.n;
-    const uint32_t ru = btree_o_rank(S, u);
-    // the tile's positions and its scratch, indexed from the tile start
-    K *At = A + P0;
-    const K *St = scr + btree_o_soff(S, u) + P0;
-    for (uint64_t a = P0; a < P1;) {
-        uint32_t lv;
-        uint64_t e;
-        btree_fix_piece(S, a, P1, lv, e);
-        const uint64_t z0 = btree_src_rank_at(S, lv, a) >> S.tile_shift;
-        const uint64_t z1 = btree_src_rank_at(S, lv, e - 1) >> S.tile_shift;
-        const uint32_t ea = (uint32_t)(a - P0), ee = (uint32_t)(e - P0);
-        if (z1 - z0 < kFixDense) {
-            bool all = true;  // every source run of the piece went to scratch: one range
-            for (uint64_t z = z0 + tid; z <= z1; z += nt)
-                if (z == u || btree_o_rank(S, z) > ru) all = false;
-            if (__syncthreads_and(all)) {
-                for (uint32_t q = ea + tid; q < ee; q += nt * kFixUnr) {
-                    K v[kFixUnr];
-#pragma unroll
-                    for (int r = 0; r < kFixUnr; ++r)
-                        if (q + r * nt < ee) v[r] = __ldcs(St + q + r * nt);
-#pragma unroll
-                    for (int r = 0; r < kFixUnr; ++r)
-                        if (q + r * nt < ee) At[q + r * nt] = v[r];
-                }
-            } else {
-                for (uint64_t z = z0 + warp; z <= z1; z += nwarps) {  // a warp per source run
-                    if (z == u || btree_o_rank(S, z) > ru) continue;
-                    uint64_t pa, pe;
-                    btree_fix_run(S, lv, a, e, z0, z1, z, pa, pe);
-                    warp_copy_keys(At, St, (uint32_t)(pa - P0), (uint32_t)(pe - P0));
-                }
-            }
-        } else {
-            for (uint32_t q = ea + tid; q < ee; q += nt * kFixUnr) {
-                bool take[kFixUnr];
-                K v[kFixUnr];
-#pragma unroll
-                for (int r = 0; r < kFixUnr; ++r) {
-                    const uint32_t x = q + r * nt;
-                    take[r] = false;
-                    if (x < ee) {
-                        const uint64_t z = btree_src_rank_at(S, lv, P0 + x) >> S.tile_shift;
-                        take[r] = z != u && btree_o_rank(S, z) < ru;
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < kFixUnr; ++r)
-                    if (take[r]) v[r] = __ldcs(St + q + r * nt);
-#pragma unroll
-                for (int r = 0; r < kFixUnr; ++r)
-                    if (take[r]) At[q + r * nt] = v[r];
-            }
-        }
-        __syncthreads();  // the piece's checks are done before the next piece's
-        a = e;
     }
 }
 

@@ -72,13 +72,18 @@ btree_copy_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_con
     bulk_copy_plan(A, scr, P, stage, bars, ctrl);
 }
 
-// Second pass of a plan-O B-tree permutation for the destination tiles
-// list[0, nlist) (those not copied as whole-tile ranges): a block per tile.
+// Second pass of a plan-O B-tree permutation for the scratch keys outside the
+// whole-tile ranges: the host-listed copies, a warp per copy.
 template <typename K>
 __global__ void __launch_bounds__(kScatterThreads)
-btree_fix_kernel(K *__restrict__ A, const K *__restrict__ scr, const __grid_constant__ BtreeStream S,
-                 const uint32_t *__restrict__ list, uint64_t nlist) {
-    for (uint64_t i = blockIdx.x; i < nlist; i += gridDim.x) btree_fix_tile_block(S, A, scr, (uint64_t)__ldg(list + i));
+btree_fix_kernel(K *__restrict__ A, const K *__restrict__ scr, const FixSeg *__restrict__ segs, uint64_t nsegs) {
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w; i < nsegs; i += nw) {
+        const uint64_t dl = __ldg(reinterpret_cast<const unsigned long long *>(&segs[i].dst_len));
+        const uint64_t src = __ldg(reinterpret_cast<const unsigned long long *>(&segs[i].src));
+        warp_copy_keys(A + (dl & kSegDstMask), scr + src, 0, (uint32_t)(dl >> 48));
+    }
 }
 
 // One copy range for the bulk engine: its 16-byte-aligned interior in
@@ -409,11 +414,12 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, wc, flags);
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
-        if (pl.ordered && pl.ot.nlist) {
+        if (pl.ordered && pl.ot.nsegs) {
             int fper = 0;
             TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fper, btree_fix_kernel<K>, kScatterThreads, 0));
-            const uint64_t fg = std::min<uint64_t>(pl.ot.nlist, (uint64_t)std::max(fper, 1) * smx);
-            btree_fix_kernel<K><<<(unsigned)fg, kScatterThreads, 0, st>>>(A, scr, pl.bs, pl.ot.list, pl.ot.nlist);
+            const uint64_t fg = std::min<uint64_t>((pl.ot.nsegs * 32 + kScatterThreads - 1) / kScatterThreads,
+                                                   (uint64_t)std::max(fper, 1) * smx);
+            btree_fix_kernel<K><<<(unsigned)fg, kScatterThreads, 0, st>>>(A, scr, pl.ot.segs, pl.ot.nsegs);
             TL_CUDA_TRY(cudaGetLastError());
         }
         BulkPlan bp;
@@ -495,11 +501,7 @@ int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes,
         for (uint64_t i = 0; i < pl.ot.nranges; ++i)
             c += std::min<uint64_t>((uint64_t)pl.ot.ranges[i].y << pl.bs.tile_shift, n) -
                  ((uint64_t)pl.ot.ranges[i].x << pl.bs.tile_shift);
-        for (uint64_t i = 0; i < pl.ot.nlist; ++i)
-            btree_fix_tile_host(pl.bs, pl.ot.list[i], [&](uint64_t, uint64_t len) {
-                c += len;
-                return true;
-            });
+        for (uint64_t i = 0; i < pl.ot.nsegs; ++i) c += pl.ot.segs[i].dst_len >> 48;
         *keys = c;
     } else {
         *keys = 0;
@@ -773,22 +775,20 @@ static int emulate_permute_kb(int layout, uint64_t n, uint64_t b, uint32_t key_b
                         read_slot[sl] = 1;
                     }
                 }
-                for (uint64_t i = 0; i < pl.ot.nlist; ++i) {
-                    const uint64_t u = pl.ot.list[i];
-                    const int64_t so = btree_o_soff(pl.bs, u);
-                    btree_fix_tile_host(pl.bs, u, [&](uint64_t pa, uint64_t len) {
-                        for (uint64_t d = pa; d < pa + len; ++d) {
-                            const uint64_t sl = d + (uint64_t)so;
-                            if (d >= n || sl >= pl.bs.nscratch || slot_writes[sl] != 1 || read_slot[sl]) {
-                                ++viol;
-                                continue;
-                            }
-                            A[d] = scr[sl];
-                            ++pos_writes[d];
-                            read_slot[sl] = 1;
+                for (uint64_t i = 0; i < pl.ot.nsegs; ++i) {
+                    const uint64_t d0 = pl.ot.segs[i].dst_len & kSegDstMask, len = pl.ot.segs[i].dst_len >> 48;
+                    for (uint64_t e = 0; e < len; ++e) {
+                        const uint64_t d = d0 + e, sl = pl.ot.segs[i].src + e;
+                        // a copy takes the slot of its own position
+                        if (d >= n || sl >= pl.bs.nscratch || slot_writes[sl] != 1 || read_slot[sl] ||
+                            sl != d + (uint64_t)btree_o_soff(pl.bs, d / pl.tile_keys)) {
+                            ++viol;
+                            continue;
                         }
-                        return true;
-                    });
+                        A[d] = scr[sl];
+                        ++pos_writes[d];
+                        read_slot[sl] = 1;
+                    }
                 }
                 for (uint64_t c = 0; c < pl.bs.nscratch; ++c)
                     if (slot_writes[c] != read_slot[c]) ++viol;
