@@ -155,7 +155,7 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
                      const uint32_t *__restrict__ owner, BatchTotals tot, Ctrl *ctrl, WaitCfg wc,
                      unsigned int *flags, unsigned int *done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K *sm = reinterpret_cast<K *>(smem_raw);
+    K *sm = tile_smem<K>(smem_raw);
     __shared__ unsigned long long s_ticket;
     __shared__ int s_ok;
     __shared__ uint32_t s_j;
@@ -437,7 +437,7 @@ static int launch_batch_permute(const tl_batch_plan_impl &P, K *keys, char *ws, 
     wc.flag_value = 1;
     wc.wait_value = debug_force_timeout() ? 0xFFFFFFFFu : 1u;
     wc.spin_limit = debug_spin_limit();
-    const size_t smem = (size_t)P.tot.max_tile * sizeof(K) + 16;  // the largest tile plus its 16-byte head slack
+    const size_t smem = (size_t)P.tot.max_tile * sizeof(K) + kTileSmemSlack;  // the largest tile
     auto kern = batch_permute_kernel<K>;
     TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;

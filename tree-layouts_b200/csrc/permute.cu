@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kStreamThreads, kStreamBlocksPerSM)
 btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant__ BtreeStream S, Ctrl *ctrl,
                     WaitCfg wc, unsigned int *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K *sm = reinterpret_cast<K *>(smem_raw);
+    K *sm = tile_smem<K>(smem_raw);
     __shared__ unsigned long long s_ticket;
     __shared__ TileShared ts;
     TicketPipe tp;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kStreamThreads, kStreamBlocksPerSM)
 mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant__ MvebParams prm,
                    Ctrl *ctrl, WaitCfg wc, unsigned int *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K *sm = reinterpret_cast<K *>(smem_raw);
+    K *sm = reinterpret_cast<K *>(smem_raw);  // see load_tile_issue
     __shared__ unsigned long long s_ticket;
     __shared__ int s_ok;
     __shared__ unsigned char s_inv[256];
@@ -226,7 +226,7 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
             loaded_U = R.U;
         }
         if (threadIdx.x == 0) s_ok = 1;  // the previous tile's readers are past the ticket barrier
-        const uint64_t base = load_tile(A, p0, p1, sm);
+        const uint64_t base = load_tile<16>(A, p0, p1, sm);
         publish_read(&flags[k], wc);
         if (R.U == 0) {
             for (uint64_t x = p0 + threadIdx.x; x < p1; x += blockDim.x)
@@ -385,7 +385,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
     wc.spin_limit = debug_spin_limit();
     // flags and control block are contiguous: one stream-ordered memset clears both
     TL_CUDA_TRY(cudaMemsetAsync(flags, 0, pl.bytes - pl.off_flags, st));
-    const size_t smem = (size_t)pl.tile_keys * sizeof(K) + 16;  // the tile plus its 16-byte head slack
+    const size_t smem = (size_t)pl.tile_keys * sizeof(K) + kTileSmemSlack;
     const int smx = sm_count();
     if (is_veb_layout(pl.layout)) {
         auto kern = mveb_stream_kernel<K>;
@@ -463,7 +463,7 @@ int btree_plan_of(uint64_t n, uint64_t b) {
 }
 
 int stream_blocks_per_sm(int layout, uint32_t key_bytes) {
-    const size_t smem = 32768 + 16;
+    const size_t smem = 32768 + kTileSmemSlack;
     int per_sm = 0;
     cudaError_t e;
     if (is_veb_layout(layout))

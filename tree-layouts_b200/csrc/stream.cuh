@@ -100,31 +100,48 @@ __device__ __forceinline__ unsigned long long ticket_advance(const TicketPipe &t
     return *s_ticket;
 }
 
-// Copies src[p0, p1) into shared memory so that element x sits at
-// sm[x - base], base = p0 rounded down to a 16-byte boundary of the global
-// address.  Returns base when the copy has landed.  The 16-byte-aligned interior
-// goes through cp.async (global -> shared without registers), so every thread
-// has all of its copies in flight at once; the ragged ends use plain loads.
-// The base of load_tile for a tile starting at p0.
+// Bytes of dynamic shared memory a tile kernel asks for beyond its tile: room
+// to start the buffer on a 128-byte line, and the tile's head of up to 128
+// bytes (see load_tile_issue).
+constexpr size_t kTileSmemSlack = 128 + 128;
+
+// The tile buffer of a tile kernel: its dynamic shared memory rounded up to a
+// 128-byte line (whatever the static shared memory before it).
 template <typename K>
-__device__ __forceinline__ uint64_t tile_base(const K *src, uint64_t p0) {
-    return p0 - (reinterpret_cast<uintptr_t>(src + p0) & 15) / sizeof(K);
+__device__ __forceinline__ K *tile_smem(unsigned char *dyn) {
+    return reinterpret_cast<K *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~(uintptr_t)127);
 }
 
-// load_tile in two halves: issue returns base with the interior's copies still
-// in flight; load_tile_wait waits for them.  Threads tid of nt (default: the
-// whole block) share the copies.
-template <typename K>
+// The base of load_tile for a tile starting at p0: p0 rounded down to a
+// Line-byte boundary of the global address (Line = 128 for a buffer from
+// tile_smem, 16 for one that keeps its own placement).
+template <uint32_t Line = 128, typename K>
+__device__ __forceinline__ uint64_t tile_base(const K *src, uint64_t p0) {
+    return p0 - (reinterpret_cast<uintptr_t>(src + p0) & (Line - 1)) / sizeof(K);
+}
+
+// Copies src[p0, p1) into shared memory so that element x sits at
+// sm[x - base], base = tile_base<Line>(src, p0).  With Line = 128 and a
+// line-aligned buffer the copy keeps each key's offset within its 128-byte
+// line, so a warp's 16-byte cp.async chunks (global -> shared without
+// registers, every thread with all of its copies in flight) fill whole sectors
+// on both sides; shifted against the line, each chunk fetches its own 32-byte
+// sector, twice the L2 traffic.  (The vEB stream kernel measured faster with
+// its buffer where the static shared memory leaves it and Line = 16.)  The
+// ragged ends use plain loads.  In two halves: issue returns base with the
+// interior's copies still in flight, load_tile_wait waits for them.  Threads
+// tid of nt (default: the whole block) share the copies.
+template <uint32_t Line = 128, typename K>
 __device__ __forceinline__ uint64_t load_tile_issue(const K *__restrict__ src, uint64_t p0, uint64_t p1, K *sm,
                                                     uint32_t tid = threadIdx.x, uint32_t nt = blockDim.x) {
     constexpr uint32_t V = 16 / sizeof(K);
-    uintptr_t addr0 = reinterpret_cast<uintptr_t>(src + p0);
-    uint64_t head = (addr0 & 15) / sizeof(K);  // elements before the 16-byte boundary
-    uint64_t base = p0 - head;
-    uint64_t a0 = head ? p0 + (V - head) : p0;  // first aligned element
+    const uintptr_t addr0 = reinterpret_cast<uintptr_t>(src + p0);
+    const uint64_t base = tile_base<Line>(src, p0);
+    const uint64_t head = (addr0 & 15) / sizeof(K);  // elements before the 16-byte boundary
+    uint64_t a0 = head ? p0 + (V - head) : p0;      // first aligned element
     if (a0 > p1) a0 = p1;
-    uint64_t nvec = (p1 - a0) / V;
-    uint64_t a1 = a0 + nvec * V;
+    const uint64_t nvec = (p1 - a0) / V;
+    const uint64_t a1 = a0 + nvec * V;
     for (uint64_t x = p0 + tid; x < a0; x += nt) sm[x - base] = src[x];
     const char *gsrc = reinterpret_cast<const char *>(src + a0);
     const uint32_t sdst = (uint32_t)__cvta_generic_to_shared(sm + (a0 - base));
@@ -138,9 +155,9 @@ __device__ __forceinline__ uint64_t load_tile_issue(const K *__restrict__ src, u
 
 __device__ __forceinline__ void load_tile_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <typename K>
+template <uint32_t Line = 128, typename K>
 __device__ __forceinline__ uint64_t load_tile(const K *__restrict__ src, uint64_t p0, uint64_t p1, K *sm) {
-    const uint64_t base = load_tile_issue(src, p0, p1, sm);
+    const uint64_t base = load_tile_issue<Line>(src, p0, p1, sm);
     load_tile_wait();
     return base;
 }
