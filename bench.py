@@ -407,9 +407,11 @@ def run_ours(args, rank, world, local):
     pass2_bytes = 2.0 * skeys.value * kb
     stalls, polls = C.c_uint64(0), C.c_uint64(0)  # of the last timed permutation
     L.tl_debug_wait_stats(C.byref(stalls), C.byref(polls))
+    launches_per_step = L.tl_debug_permute_launches()
     L.tl_debug_permute_plan.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint32]
     plan = L.tl_debug_permute_plan(lay, n, b or 16, kb)
-    pass2_kernel = {0: "btree_copy_kernel", 1: "btree_copy_kernel", 2: "btree_fix_kernel"}.get(plan, "mveb_scatter_kernel")
+    pass2_kernel = {0: "btree_copy_kernel", 1: "btree_copy_kernel",
+                    2: "btree_copy_kernel + btree_fix_kernel"}.get(plan, "mveb_scatter_kernel")
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"stream_traffic_{args.workload}.json")
     if os.path.exists(prof):
@@ -509,7 +511,7 @@ def run_ours(args, rank, world, local):
             "learned": lrn,
             "batched": bat,
             "clocks": clk,
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": launches_per_step * args.steps,
         }
         print(json.dumps(line))
 

@@ -308,6 +308,8 @@ int tl_debug_btree_plan(uint64_t n, uint64_t b);
  * tl_permute_workspace_bytes: 0 right-to-left, 1 left-to-right, 2 ordered
  * tiles (B-tree and BST from 64 tiles up), 3 the vEB engine; < 0 on error. */
 int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes);
+/* Kernels the last permutation launched (stream pass and second pass). */
+int tl_debug_permute_launches(void);
 /* Resident blocks per SM of the stream kernel of `layout` at key_bytes (occupancy check). */
 int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes);
 /* fixed_only != 0: B-tree and BST permutations keep to the fixed-direction

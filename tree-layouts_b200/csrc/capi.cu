@@ -142,6 +142,8 @@ int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes
 
 int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes) { return stream_blocks_per_sm(layout, key_bytes); }
 
+int tl_debug_permute_launches(void) { return last_permute_launches(); }
+
 int tl_debug_set_schedule(int fixed_only) {
     set_fixed_schedule_only(fixed_only != 0);
     return TL_SUCCESS;

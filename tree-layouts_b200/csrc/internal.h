@@ -94,6 +94,7 @@ int btree_plan_of(uint64_t n, uint64_t b);
 int permute_plan_of(int layout, uint64_t n, uint64_t b, uint32_t key_bytes);
 void set_fixed_schedule_only(bool on);
 int stream_blocks_per_sm(int layout, uint32_t key_bytes);
+int last_permute_launches();
 int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
 int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations);
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,

@@ -373,8 +373,23 @@ static int sm_count() {
     return g_sm_count;
 }
 
+static std::atomic<int> g_last_launches{0};  // kernels the last permutation launched (profiling hook)
+
+int last_permute_launches() { return g_last_launches; }
+
+template <typename K>
+static int launch_permute_k(const PermutePlan &pl, K *A, char *ws, cudaStream_t st, EventTimer &timer, int &nl);
+
 template <typename K>
 static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st, EventTimer &timer) {
+    int nl = 0;
+    const int rc = launch_permute_k(pl, A, ws, st, timer, nl);
+    g_last_launches = nl;
+    return rc;
+}
+
+template <typename K>
+static int launch_permute_k(const PermutePlan &pl, K *A, char *ws, cudaStream_t st, EventTimer &timer, int &nl) {
     // the scratch shares A's offset within 16 bytes, so the copy pass vectorises
     K *scr = reinterpret_cast<K *>(ws + (reinterpret_cast<uintptr_t>(A) & 15));
     unsigned int *flags = reinterpret_cast<unsigned int *>(ws + pl.off_flags);
@@ -393,7 +408,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         int per_sm = 0;
         TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
         uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * smx, std::max<uint64_t>(pl.ntiles, 1));
-        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.mp, ctrl, wc, flags);
+        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.mp, ctrl, wc, flags), ++nl;
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
         if (pl.scratch_keys) {
@@ -403,6 +418,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
             uint64_t sg = std::min<uint64_t>((pl.scratch_keys + kScatterThreads - 1) / kScatterThreads,
                                              (uint64_t)std::max(sper, 1) * smx);
             mveb_scatter_kernel<K><<<(unsigned)sg, kScatterThreads, 0, st>>>(A, scr, pl.mp);
+            ++nl;
             TL_CUDA_TRY(cudaGetLastError());
         }
     } else {
@@ -411,7 +427,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
         int per_sm = 0;
         TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
         uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * smx, std::max<uint64_t>(pl.ntiles, 1));
-        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, wc, flags);
+        if (pl.ntiles) kern<<<(unsigned)grid, kStreamThreads, smem, st>>>(A, scr, pl.bs, ctrl, wc, flags), ++nl;
         TL_CUDA_TRY(cudaGetLastError());
         timer.mid();
         if (pl.ordered && pl.ot.nsegs) {
@@ -420,6 +436,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
             const uint64_t fg = std::min<uint64_t>((pl.ot.nsegs * 32 + kScatterThreads - 1) / kScatterThreads,
                                                    (uint64_t)std::max(fper, 1) * smx);
             btree_fix_kernel<K><<<(unsigned)fg, kScatterThreads, 0, st>>>(A, scr, pl.ot.segs, pl.ot.nsegs);
+            ++nl;
             TL_CUDA_TRY(cudaGetLastError());
         }
         BulkPlan bp;
@@ -434,6 +451,7 @@ static int launch_permute(const PermutePlan &pl, K *A, char *ws, cudaStream_t st
             TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cper, ck, 32, smem));
             const uint64_t cg = std::max<uint64_t>(1, std::min<uint64_t>(bp.nchunks, (uint64_t)std::max(cper, 1) * smx));
             ck<<<(unsigned)cg, 32, smem, st>>>(A, scr, bp, ctrl);
+            ++nl;
             TL_CUDA_TRY(cudaGetLastError());
         }
     }
