@@ -115,6 +115,16 @@ int tl_permute_veb_std_u64(uint64_t *dev_A, uint64_t n, void *stream, float *ms)
 int tl_permute_static_ws(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                          void *stream);
 
+/* The reverse permutation: a layout of n sorted keys (as tl_permute leaves it,
+ * same layout, b and key width) back to sorted order, in place.  No counterpart
+ * in the reference, whose README describes conversions between sorted order and
+ * the layouts but implements only sorted -> layout.  Workspace, stream and ms
+ * as for tl_permute (dev_workspace NULL: stream-ordered allocation of
+ * tl_unpermute_workspace_bytes, a copy of the array). */
+int tl_unpermute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
+int tl_unpermute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_workspace,
+                 uint64_t workspace_bytes, void *stream, float *ms);
+
 /* ---------------------------------------------------------------- mvEB tables */
 /* buildTable(vEB_table *table, uint64_t n, uint32_t d, uint32_t root_depth):
  * gpu/src/query-mveb.cu:25-47.  Host function; table holds d entries, zeroed by
@@ -298,6 +308,8 @@ int tl_debug_set_wait(unsigned int spin_limit, int force_timeout);
  * protocol breaches (stale read, unguarded store, bad wait, position or scratch
  * slot not written exactly once). */
 int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations);
+/* Host replay of tl_unpermute's gather on n 64-bit words (test hook). */
+int tl_debug_emulate_unpermute(int layout, uint64_t n, uint64_t b, uint64_t *host_A);
 /* sizeof of the ABI structs, for bindings to check their mirrors:
  * 0 tl_veb_table, 1 tl_rank_model, 2 tl_rank_leaf, 3 tl_rank_train_config. */
 int tl_debug_struct_size(int which);

@@ -112,3 +112,14 @@ def test_ordered_schedule_replay_at_scale(layout, n, b):
     got, viol = T.emulate_permute(layout, keys, b)
     assert viol == 0
     assert np.array_equal(got, O.permute(layout, keys, b))
+
+
+@pytest.mark.parametrize("layout,b", [("bst", 1), ("btree", 2), ("btree", 3), ("btree", 8), ("btree", 16),
+                                      ("btree", 31), ("mveb", 0), ("veb", 0)])
+def test_unpermute_replay_matches_oracle(layout, b):
+    """The reverse permutation's gather, replayed on the host with the kernels'
+    per-tile helpers, turns the oracle's layout back into sorted order."""
+    for n in SIZES:
+        keys = np.arange(n, dtype=np.uint64) * 5 + 11
+        got = T.emulate_unpermute(layout, O.permute(layout, keys, b or 16), b or 16)
+        assert np.array_equal(got, keys), (layout, b, n)

@@ -8,6 +8,7 @@
 #include "internal.h"
 #include "learned.h"
 #include "stream.cuh"
+#include "unpermute.h"
 #include "batched.h"
 
 namespace tl {
@@ -138,6 +139,19 @@ int tl_debug_btree_plan(uint64_t n, uint64_t b) { return btree_plan_of(n, b); }
 
 int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes) {
     return permute_plan_of(layout, n, b, key_bytes);
+}
+
+int tl_unpermute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_workspace,
+                 uint64_t workspace_bytes, void *stream, float *ms) {
+    return unpermute(layout, dev_A, n, b, key_bytes, dev_workspace, workspace_bytes, S(stream), ms);
+}
+
+int tl_unpermute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes) {
+    return unpermute_workspace_bytes(layout, n, b, key_bytes, bytes);
+}
+
+int tl_debug_emulate_unpermute(int layout, uint64_t n, uint64_t b, uint64_t *host_A) {
+    return emulate_unpermute(layout, n, b, host_A);
 }
 
 int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes) { return stream_blocks_per_sm(layout, key_bytes); }

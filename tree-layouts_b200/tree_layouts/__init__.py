@@ -62,6 +62,9 @@ def lib():
         L.tl_permute_workspace_bytes.argtypes = [C.c_int, _u64, _u64, _u32, C.POINTER(_u64)]
         L.tl_layout_position.argtypes = [C.c_int, _u64, _u64, _u64, C.POINTER(_u64)]
         L.tl_debug_emulate_permute.argtypes = [C.c_int, _u64, _u64, _v, C.POINTER(_u64)]
+        L.tl_debug_emulate_unpermute.argtypes = [C.c_int, _u64, _u64, _v]
+        L.tl_unpermute.argtypes = [C.c_int, _v, _u64, _u64, _u32, _v, _u64, _v, _f32p]
+        L.tl_unpermute_workspace_bytes.argtypes = [C.c_int, _u64, _u64, _u32, C.POINTER(_u64)]
         L.tl_debug_set_wait.argtypes = [C.c_uint, C.c_int]
         L.tl_build_table.argtypes = [_v, _u64, _u32, _u32]
         L.tl_build_table.restype = None
@@ -122,6 +125,14 @@ def emulate_permute(layout: str, keys: np.ndarray, b: int = 16):
     return A, viol.value
 
 
+def emulate_unpermute(layout: str, A: np.ndarray, b: int = 16) -> np.ndarray:
+    """Host replay of the reverse permutation's gather; returns the sorted array."""
+    out = np.ascontiguousarray(A, dtype=np.uint64).copy()
+    _check(lib().tl_debug_emulate_unpermute(LAYOUTS[layout], len(out), b, out.ctypes.data),
+           "tl_debug_emulate_unpermute")
+    return out
+
+
 def workspace_bytes(layout: str, n: int, b: int = 16, key_bytes: int = 8) -> int:
     out = _u64()
     _check(lib().tl_permute_workspace_bytes(LAYOUTS[layout], n, b, key_bytes, C.byref(out)),
@@ -165,6 +176,18 @@ def permute(layout: str, keys, b: int = 16, stream=None, workspace=None, timed: 
     rc = lib().tl_permute(LAYOUTS[layout], keys.data_ptr(), keys.numel(), b, _key_bytes(keys),
                           ws_ptr or None, ws_bytes, _stream_ptr(stream), C.byref(ms) if timed else None)
     _check(rc, f"tl_permute({layout}, n={keys.numel()})")
+    return ms.value if timed else None
+
+
+def unpermute(layout: str, keys, b: int = 16, stream=None, workspace=None, timed: bool = False):
+    """Permute a CUDA tensor holding `layout` (as permute leaves it) back to
+    sorted order in place.  Returns device ms when timed, else None."""
+    ms = C.c_float(0.0)
+    ws_ptr, ws_bytes = (0, 0) if workspace is None else (workspace.data_ptr(), workspace.numel()
+                                                           * workspace.element_size())
+    rc = lib().tl_unpermute(LAYOUTS[layout], keys.data_ptr(), keys.numel(), b, _key_bytes(keys),
+                            ws_ptr or None, ws_bytes, _stream_ptr(stream), C.byref(ms) if timed else None)
+    _check(rc, f"tl_unpermute({layout}, n={keys.numel()})")
     return ms.value if timed else None
 
 
