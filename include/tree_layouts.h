@@ -106,8 +106,9 @@ int tl_permute_veb_std_u64(uint64_t *dev_A, uint64_t n, void *stream, float *ms)
  * latency-bound service that must not hit cudaMalloc's implicit synchronisation
  * mid-request): the workspace is a fixed array of TL_STATIC_WORKSPACE_BYTES
  * compiled into the library, present on every GPU that loads it until the
- * process exits.  Permutations whose tl_permute_workspace_bytes exceeds it
- * return TL_ERROR_UNSUPPORTED.  All calls share that array: calls that overlap
+ * process exits.  It keeps to the fixed-direction schedules (the ordered one
+ * needs per-size tables the library would allocate); permutations whose
+ * workspace under those exceeds the array return TL_ERROR_UNSUPPORTED.  All calls share that array: calls that overlap
  * on the GPU race, so serialise them.  The first call on a device looks the
  * array up (cudaGetSymbolAddress); make it before any stream capture.
  * Synchronous like tl_permute; allocates nothing. */

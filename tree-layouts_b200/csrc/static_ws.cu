@@ -12,9 +12,10 @@
 //
 // Limits and sharing:
 //  - The array is kStaticWorkspaceBytes (32 MiB) on every GPU that loads the
-//    library, held until the process exits.  A permutation whose workspace
-//    (tl_permute_workspace_bytes) exceeds it is rejected with
-//    TL_ERROR_UNSUPPORTED before any device work.
+//    library, held until the process exits.  The permutation keeps to the
+//    fixed-direction schedules (the ordered one keeps per-size tables that the
+//    library would allocate); one whose workspace under them exceeds the array
+//    is rejected with TL_ERROR_UNSUPPORTED before any device work.
 //  - Every call uses the same array and it keeps the previous call's contents.
 //    The permutation clears what must start at zero (the read flags, by a
 //    stream-ordered memset, and the control block, by a copy) on every call.
