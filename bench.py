@@ -418,6 +418,42 @@ def run_ours(args, rank, world, local):
         with open(prof) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
 
+    # the reverse permutation (layout -> sorted order) of the same array, device time
+    rinfo = None
+    if args.reverse:
+        layout_copy = A.clone()
+        ws = torch.empty(max(1, T.unpermute_workspace_bytes(layout, n, b or 16, kb)), dtype=torch.uint8, device=dev)
+        rms = []
+        for i in range(args.warmup + min(args.steps, 5)):
+            A.copy_(layout_copy)  # untimed
+            r = T.unpermute(layout, A, b or 16, workspace=ws, timed=True)
+            if i >= args.warmup:
+                rms.append(r)
+        assert torch.equal(A, pristine), "reverse permutation check failed"
+        r_med = statistics.median(rms)
+        rinfo = {"kernel": "device copy + " + ("veb_gather_kernel" if layout in ("mveb", "veb") else "btree_gather_kernel"),
+                 "ms": round(r_med, 4), "GBps": round(bytes_step / (r_med * 1e-3) / 1e9, 1),
+                 "frac_of_peak": round(bytes_step / (r_med * 1e-3) / 1e9 / peak, 4),
+                 "note": "2*n*w / device time; the pass moves 4*n*w (a copy to the workspace, then the gather)"}
+        del layout_copy, ws
+        A.copy_(pristine)
+        T.permute(layout, A, b or 16)  # the layout again, for the queries below
+
+    # the reference's algorithm family as a variant (BST: involutions), device time
+    vinfo = None
+    if args.variants and layout == "bst":
+        vms = []
+        for i in range(2 + 3):
+            A.copy_(pristine)  # untimed
+            r = T.permute_algorithm("bst", "involutions", A, 1, timed=True)
+            if i >= 2:
+                vms.append(r)
+        v_med = statistics.median(vms)
+        vinfo = {"involutions": {"ms": round(v_med, 4), "GBps": round(bytes_step / (v_med * 1e-3) / 1e9, 1),
+                                 "kernels": "bitrev + lowrev swaps (+ 2 involutions and 3 reversals if non-perfect)"}}
+        A.copy_(pristine)
+        T.permute(layout, A, b or 16)  # the library's layout again, for the queries below
+
     # plain B-tree / BST / mvEB queries on the permuted layout (device time)
     qinfo = None
     if args.queries and q:
@@ -507,6 +543,8 @@ def run_ours(args, rank, world, local):
                          "whole_permute_frac": round(bytes_step / (ms_local * 1e-3) / 1e9 / peak, 4)},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "reverse": rinfo,
+            "variants": vinfo,
             "queries": qinfo,
             "learned": lrn,
             "batched": bat,
@@ -525,6 +563,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--n", type=int, default=0, help="override n (profiling runs)")
     ap.add_argument("--queries", type=int, default=1)
+    ap.add_argument("--reverse", type=int, default=1, help="reverse permutation (layout -> sorted) section")
+    ap.add_argument("--variants", type=int, default=1, help="the reference's algorithm family as a variant (BST)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=50_000_000)
     ap.add_argument("--ref-n", type=int, default=0, help="reference arm keys (0: the workload's full n)")

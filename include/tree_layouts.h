@@ -116,6 +116,18 @@ int tl_permute_veb_std_u64(uint64_t *dev_A, uint64_t n, void *stream, float *ms)
 int tl_permute_static_ws(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                          void *stream);
 
+/* The reference's algorithm families as variants of tl_permute (its library
+ * ships several for each layout: cycle-leader, involutions, hybrid):
+ * TL_ALGO_STREAM is this library's own single-pass stream permutation (what
+ * tl_permute runs); TL_ALGO_INVOLUTIONS the BST by involutions
+ * (gpu/src/bst-involutions.cuh:168-195 timePermuteBST), for ablations and as a
+ * second route to the same layout.  Other (layout, algorithm) pairs return
+ * TL_ERROR_UNSUPPORTED.  Allocates nothing beyond what tl_permute does;
+ * synchronous; ms as for tl_permute. */
+typedef enum { TL_ALGO_STREAM = 0, TL_ALGO_INVOLUTIONS = 1 } tl_algorithm;
+int tl_permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
+                         void *stream, float *ms);
+
 /* The reverse permutation: a layout of n sorted keys (as tl_permute leaves it,
  * same layout, b and key width) back to sorted order, in place.  No counterpart
  * in the reference, whose README describes conversions between sorted order and

@@ -141,6 +141,11 @@ int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes
     return permute_plan_of(layout, n, b, key_bytes);
 }
 
+int tl_permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
+                         void *stream, float *ms) {
+    return permute_algorithm(layout, algorithm, dev_A, n, b, key_bytes, S(stream), ms);
+}
+
 int tl_unpermute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_workspace,
                  uint64_t workspace_bytes, void *stream, float *ms) {
     return unpermute(layout, dev_A, n, b, key_bytes, dev_workspace, workspace_bytes, S(stream), ms);

@@ -92,6 +92,8 @@ int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_byt
 int permute_workspace_bytes_fixed(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
 int btree_plan_of(uint64_t n, uint64_t b);
 int permute_plan_of(int layout, uint64_t n, uint64_t b, uint32_t key_bytes);
+int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
+                      cudaStream_t st, float *ms);
 void set_fixed_schedule_only(bool on);
 int stream_blocks_per_sm(int layout, uint32_t key_bytes);
 int last_permute_launches();

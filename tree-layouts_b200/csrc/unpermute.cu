@@ -141,12 +141,17 @@ veb_gather_kernel(K *__restrict__ A, const K *__restrict__ C, const __grid_const
             const uint64_t u = (1ull << U) - 1;
             uint64_t g0, g1;
             mveb_tile_groups(R, p0, p1, g0, g1);
+            // the separators (each a position search of its own): a thread per unit
+            for (uint64_t gi = g0 + threadIdx.x; gi < g1; gi += blockDim.x) {
+                const uint64_t first = R.src + (gi << U);
+                if (first + u < R.src + R.len) sm[first - p0 + u] = C[veb_pos(P.n, first + u, modified)];
+            }
+            // the units' bodies: a warp per unit, contiguous reads
             for (uint64_t gi = g0 + warp; gi < g1; gi += nwarps) {
                 const uint64_t first = R.src + (gi << U);  // sorted rank of the unit's first key
                 const uint32_t o = (uint32_t)(first - p0);
                 const uint64_t dst = mveb_unit_dst(R, gi);
                 for (uint32_t q = lane; q < u; q += 32) sm[o + s_inv[q]] = C[dst + q];
-                if (lane == 0 && first + u < R.src + R.len) sm[o + u] = C[veb_pos(P.n, first + u, modified)];
             }
         }
         __syncthreads();

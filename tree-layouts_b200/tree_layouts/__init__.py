@@ -64,6 +64,7 @@ def lib():
         L.tl_debug_emulate_permute.argtypes = [C.c_int, _u64, _u64, _v, C.POINTER(_u64)]
         L.tl_debug_emulate_unpermute.argtypes = [C.c_int, _u64, _u64, _v]
         L.tl_unpermute.argtypes = [C.c_int, _v, _u64, _u64, _u32, _v, _u64, _v, _f32p]
+        L.tl_permute_algorithm.argtypes = [C.c_int, C.c_int, _v, _u64, _u64, _u32, _v, _f32p]
         L.tl_unpermute_workspace_bytes.argtypes = [C.c_int, _u64, _u64, _u32, C.POINTER(_u64)]
         L.tl_debug_set_wait.argtypes = [C.c_uint, C.c_int]
         L.tl_build_table.argtypes = [_v, _u64, _u32, _u32]
@@ -133,6 +134,13 @@ def emulate_unpermute(layout: str, A: np.ndarray, b: int = 16) -> np.ndarray:
     return out
 
 
+def unpermute_workspace_bytes(layout: str, n: int, b: int = 16, key_bytes: int = 8) -> int:
+    out = _u64()
+    _check(lib().tl_unpermute_workspace_bytes(LAYOUTS[layout], n, b, key_bytes, C.byref(out)),
+           "tl_unpermute_workspace_bytes")
+    return out.value
+
+
 def workspace_bytes(layout: str, n: int, b: int = 16, key_bytes: int = 8) -> int:
     out = _u64()
     _check(lib().tl_permute_workspace_bytes(LAYOUTS[layout], n, b, key_bytes, C.byref(out)),
@@ -176,6 +184,19 @@ def permute(layout: str, keys, b: int = 16, stream=None, workspace=None, timed: 
     rc = lib().tl_permute(LAYOUTS[layout], keys.data_ptr(), keys.numel(), b, _key_bytes(keys),
                           ws_ptr or None, ws_bytes, _stream_ptr(stream), C.byref(ms) if timed else None)
     _check(rc, f"tl_permute({layout}, n={keys.numel()})")
+    return ms.value if timed else None
+
+
+ALGORITHMS = {"stream": 0, "involutions": 1}
+
+
+def permute_algorithm(layout: str, algorithm: str, keys, b: int = 16, stream=None, timed: bool = False):
+    """tl_permute_algorithm: the layout by one of the reference's algorithm
+    families ("involutions": BST only) or by this library's own ("stream")."""
+    ms = C.c_float(0.0)
+    rc = lib().tl_permute_algorithm(LAYOUTS[layout], ALGORITHMS[algorithm], keys.data_ptr(), keys.numel(), b,
+                                    _key_bytes(keys), _stream_ptr(stream), C.byref(ms) if timed else None)
+    _check(rc, f"tl_permute_algorithm({layout}, {algorithm}, n={keys.numel()})")
     return ms.value if timed else None
 
 
