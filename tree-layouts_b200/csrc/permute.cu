@@ -185,12 +185,20 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
         uint64_t g0, g1;
         mveb_tile_groups(R, p0, p1, g0, g1);
         const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-        for (uint64_t gi = g0 + warp; gi < g1; gi += nwarps) {
-            const uint32_t gsrc = (uint32_t)(R.src + (gi << U) - base);
-            const uint64_t dst = mveb_unit_dst(R, gi);
-            for (uint32_t q = lane; q < u; q += 32) A[dst + q] = sm[gsrc + s_inv[q]];
-            if (lane == 0 && R.src + (gi << U) + u < R.src + R.len)
-                scr[R.slot_base + gi] = sm[gsrc + u];
+        // a warp's units in batches of 32: their destinations lane-parallel, one
+        // unit per lane, then each unit's keys by the whole warp
+        for (uint64_t gb = g0 + warp; gb < g1; gb += 32ull * nwarps) {
+            const uint64_t gl = gb + (uint64_t)lane * nwarps;
+            const uint64_t my_dst = gl < g1 ? mveb_unit_dst(R, gl) : 0;
+            const uint32_t nb = (uint32_t)std::min<uint64_t>(32, (g1 - gb + nwarps - 1) / nwarps);
+            for (uint32_t j = 0; j < nb; ++j) {
+                const uint64_t gi = gb + (uint64_t)j * nwarps;
+                const uint64_t dst = __shfl_sync(0xFFFFFFFFu, my_dst, j);
+                const uint32_t gsrc = (uint32_t)(R.src + (gi << U) - base);
+                for (uint32_t q = lane; q < u; q += 32) A[dst + q] = sm[gsrc + s_inv[q]];
+                if (lane == 0 && R.src + (gi << U) + u < R.src + R.len)
+                    scr[R.slot_base + gi] = sm[gsrc + u];
+            }
         }
     }
 }

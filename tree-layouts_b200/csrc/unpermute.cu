@@ -146,12 +146,18 @@ veb_gather_kernel(K *__restrict__ A, const K *__restrict__ C, const __grid_const
                 const uint64_t first = R.src + (gi << U);
                 if (first + u < R.src + R.len) sm[first - p0 + u] = C[veb_pos(P.n, first + u, modified)];
             }
-            // the units' bodies: a warp per unit, contiguous reads
-            for (uint64_t gi = g0 + warp; gi < g1; gi += nwarps) {
-                const uint64_t first = R.src + (gi << U);  // sorted rank of the unit's first key
-                const uint32_t o = (uint32_t)(first - p0);
-                const uint64_t dst = mveb_unit_dst(R, gi);
-                for (uint32_t q = lane; q < u; q += 32) sm[o + s_inv[q]] = C[dst + q];
+            // the units' bodies: a warp per unit, contiguous reads; a warp's units
+            // in batches of 32, their positions lane-parallel
+            for (uint64_t gb = g0 + warp; gb < g1; gb += 32ull * nwarps) {
+                const uint64_t gl = gb + (uint64_t)lane * nwarps;
+                const uint64_t my_dst = gl < g1 ? mveb_unit_dst(R, gl) : 0;
+                const uint32_t nb = (uint32_t)min((uint64_t)32, (g1 - gb + nwarps - 1) / nwarps);
+                for (uint32_t j = 0; j < nb; ++j) {
+                    const uint64_t gi = gb + (uint64_t)j * nwarps;
+                    const uint64_t dst = __shfl_sync(0xFFFFFFFFu, my_dst, j);
+                    const uint32_t o = (uint32_t)(R.src + (gi << U) - p0);
+                    for (uint32_t q = lane; q < u; q += 32) sm[o + s_inv[q]] = C[dst + q];
+                }
             }
         }
         __syncthreads();
