@@ -337,6 +337,7 @@ def batched_section(args, dev):
            "permute_frac_of_peak": round(2.0 * total * 8 / (pm * 1e-3) / 1e9 / peaks()[0], 4),
            "queries": Q.numel(), "query_ms": round(qms, 3), "queries_per_s": round(Q.numel() / (qms * 1e-3), 1),
            "autotune_s": round(tune_s, 2), "tuning": {k: report[k] for k in ("threads", "query_chunk")},
+           "ordered_instances": plan.ordered()[0], "ordered_keys": plan.ordered()[1],
            "instances_checked": checked}
     del keys, pristine, Q, inst, ans, ws
     torch.cuda.empty_cache()

@@ -337,9 +337,15 @@ int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes
 int tl_debug_permute_launches(void);
 /* Resident blocks per SM of the stream kernel of `layout` at key_bytes (occupancy check). */
 int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes);
-/* fixed_only != 0: B-tree and BST permutations keep to the fixed-direction
- * schedules (0 and 1 of tl_debug_permute_plan); 0 restores the default. */
-int tl_debug_set_schedule(int fixed_only);
+/* mode 1: B-tree and BST permutations keep to the fixed-direction schedules
+ * (0 and 1 of tl_debug_permute_plan), batched plans built from then on too;
+ * mode 2: batched plans built from then on put every instance the ordered
+ * schedule applies to on it, whatever it saves; 0 restores the default. */
+int tl_debug_set_schedule(int mode);
+/* Instances of a batched plan on the ordered-tile schedule and their keys: by
+ * default those of 64 tiles or more (at the plan's tile size for their size
+ * class) whose scratch keys it cuts to 30 % or less. */
+int tl_debug_batch_ordered(const tl_batch_plan *plan, uint64_t *instances, uint64_t *keys);
 /* Of the last permutation's bounded waits: how many found their flag unset at
  * the first look, and how many polls those took in total. */
 int tl_debug_wait_stats(uint64_t *stalled_waits, uint64_t *polls);

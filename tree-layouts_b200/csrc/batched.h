@@ -10,6 +10,7 @@ int batch_plan_destroy(tl_batch_plan *plan);
 int batch_workspace_bytes(const tl_batch_plan *plan, uint64_t *bytes);
 int batch_permute(const tl_batch_plan *plan, void *dev_keys, void *dev_ws, uint64_t ws_bytes, cudaStream_t st);
 int batch_status(const tl_batch_plan *plan, const void *dev_ws, cudaStream_t st);
+int batch_ordered(const tl_batch_plan *plan, uint64_t *instances, uint64_t *keys);
 int batch_query_workspace_bytes(const tl_batch_plan *plan, uint64_t q, uint64_t *bytes);
 int batch_query(const tl_batch_plan *plan, const void *dev_keys, const void *dev_queries, const uint32_t *dev_inst,
                 uint64_t q, uint64_t *dev_answers, void *dev_ws, uint64_t ws_bytes, cudaStream_t st, float *ms);

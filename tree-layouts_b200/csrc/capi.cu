@@ -163,8 +163,9 @@ int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes) { return strea
 
 int tl_debug_permute_launches(void) { return last_permute_launches(); }
 
-int tl_debug_set_schedule(int fixed_only) {
-    set_fixed_schedule_only(fixed_only != 0);
+int tl_debug_set_schedule(int mode) {
+    if (mode < 0 || mode > 2) return TL_ERROR_INVALID_VALUE;
+    set_schedule_mode(mode);
     return TL_SUCCESS;
 }
 
@@ -173,6 +174,10 @@ int tl_debug_wait_stats(uint64_t *stalled_waits, uint64_t *polls) {
     *stalled_waits = g_stalled_waits;
     *polls = g_stall_polls;
     return TL_SUCCESS;
+}
+
+int tl_debug_batch_ordered(const tl_batch_plan *plan, uint64_t *instances, uint64_t *keys) {
+    return batch_ordered(plan, instances, keys);
 }
 
 int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys) {

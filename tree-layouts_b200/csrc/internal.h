@@ -94,7 +94,11 @@ int btree_plan_of(uint64_t n, uint64_t b);
 int permute_plan_of(int layout, uint64_t n, uint64_t b, uint32_t key_bytes);
 int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                       cudaStream_t st, float *ms);
-void set_fixed_schedule_only(bool on);
+// Debug schedule mode (tl_debug_set_schedule): 0 default, 1 fixed directions
+// only, 2 batched plans order every instance the ordered schedule applies to.
+void set_schedule_mode(int mode);
+bool fixed_schedule_only();
+bool ordered_schedule_forced();
 int stream_blocks_per_sm(int layout, uint32_t key_bytes);
 int last_permute_launches();
 int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);

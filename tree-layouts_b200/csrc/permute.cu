@@ -243,9 +243,13 @@ struct PermutePlan {
 // ORDER_ALWAYS whenever there is a top tree and more than one tile (host replay).
 enum OrderMode { ORDER_NEVER = 0, ORDER_AUTO = 1, ORDER_ALWAYS = 2 };
 constexpr uint64_t kOrderMinTiles = 64;
-static std::atomic<int> g_fixed_only{0};  // tl_debug_set_schedule: ORDER_AUTO acts as ORDER_NEVER
+// tl_debug_set_schedule: 1 = ORDER_AUTO acts as ORDER_NEVER; 2 = batched plans
+// order every instance that can take the ordered schedule
+static std::atomic<int> g_schedule_mode{0};
 
-void set_fixed_schedule_only(bool on) { g_fixed_only = on ? 1 : 0; }
+void set_schedule_mode(int mode) { g_schedule_mode = mode; }
+bool fixed_schedule_only() { return g_schedule_mode == 1; }
+bool ordered_schedule_forced() { return g_schedule_mode == 2; }
 
 // Plan O's tables come from the library's cache unless `tables` are given.
 static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, PermutePlan &pl,
@@ -284,7 +288,7 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
         btree_choose_plan(pl.bs, key_bytes);
         if (pl.bs.g.h >= 1 && pl.ntiles >= 2 &&
             (order_mode == ORDER_ALWAYS ||
-             (order_mode == ORDER_AUTO && pl.ntiles >= kOrderMinTiles && !g_fixed_only))) {
+             (order_mode == ORDER_AUTO && pl.ntiles >= kOrderMinTiles && !fixed_schedule_only()))) {
             if (tables) pl.ot = *tables;
             if (tables || btree_order_host(pl.bs, pl.ot)) {
                 btree_set_ordered(pl.bs, pl.ot.tab, pl.ot.order, pl.ot.scratch_tiles);

@@ -29,6 +29,7 @@ def _lib():
         L.tl_batch_set_tuning.argtypes = [v, v, v, u32, u32, v, v]
         L.tl_batch_get_tuning.argtypes = [v, v, v, C.POINTER(u32), C.POINTER(u32)]
         L.tl_batch_autotune.argtypes = [v, v, v, v, v, u64, v, C.c_char_p, u64]
+        L.tl_debug_batch_ordered.argtypes = [v, C.POINTER(u64), C.POINTER(u64)]
         _bound = True
     return L
 
@@ -87,6 +88,12 @@ class BatchPlan:
                                      answers.data_ptr(), ws.data_ptr(), ws.numel(), _stream_ptr(stream),
                                      C.byref(ms) if timed else None), "tl_batch_query")
         return ms.value if timed else None
+
+    def ordered(self):
+        """(instances, keys) of the plan on the ordered-tile schedule."""
+        i, k = C.c_uint64(), C.c_uint64()
+        _check(_lib().tl_debug_batch_ordered(self.handle, C.byref(i), C.byref(k)), "tl_debug_batch_ordered")
+        return i.value, k.value
 
     def tuning(self):
         tk = (C.c_uint32 * NCLASS)()
