@@ -83,7 +83,7 @@ struct tl_batch_plan_impl {
     uint32_t query_chunk = 2048;     // queries per CTA work item
     uint32_t threads = 256;          // permute kernel block size
     uint32_t *owner = nullptr;   // device: owner instance of every tile ticket, then of every copy chunk
-    uint32_t *tloc = nullptr;    // device: the owner's own ticket of every tile ticket
+    uint32_t *tile = nullptr;    // device: the tile of its owner every tile ticket processes
     char *otab = nullptr;        // device: the ordered instances' tile tables (uint2 tab, then uint32 order)
     FixSeg *items = nullptr;     // device: the ordered instances' copy items
     uint64_t *citem = nullptr;   // device: first copy item of every copy chunk of an ordered instance
@@ -171,13 +171,15 @@ __global__ void __launch_bounds__(256) batch_setup_kernel(const int64_t *__restr
     }
 }
 
-// owner[tiles + c] = instance of copy chunk c (the tile tickets' owners come from the host).
+// owner[tiles + c] = instance of copy chunk c; tile[t], for a tile ticket t, from
+// the owner's own ticket (as the host interleaved them) to the tile it names
+// under the owner's schedule.  (The owners of tile tickets come from the host.)
 __global__ void batch_owner_kernel(const BatchInst *__restrict__ inst, uint32_t num, uint64_t tiles,
-                                   uint32_t *__restrict__ owner) {
+                                   uint32_t *__restrict__ owner, uint32_t *__restrict__ tile) {
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t j = w0; j < num; j += nw) {
+    const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, ni = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t t = i0; t < tiles; t += ni) tile[t] = (uint32_t)btree_tile_of_ticket(inst[owner[t]].S, tile[t]);
+    for (uint64_t j = i0 >> 5; j < num; j += ni >> 5) {
         const BatchInst &I = inst[j];
         for (uint64_t c = lane; c < I.nchunks; c += 32) owner[tiles + I.chunk_base + c] = (uint32_t)j;
     }
@@ -218,56 +220,105 @@ static __device__ __forceinline__ void batch_copy_ranges(K *__restrict__ keys, K
     }
 }
 
+constexpr uint32_t kNoInst = 0xFFFFFFFFu;
+constexpr uint32_t kPlanWords = sizeof(BatchInst) / 16;
+
+// Warps 1.. copy instance j's plan to a shared-memory buffer with cp.async (they
+// wait for it with their tile's copies, or explicitly after a copy chunk).
+__device__ __forceinline__ void prefetch_plan(const BatchInst *inst, uint32_t j, unsigned char *buf) {
+    if (threadIdx.x < 32) return;
+    const char *src = reinterpret_cast<const char *>(inst + j);
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(buf);
+    for (uint32_t w = threadIdx.x - 32; w < kPlanWords; w += blockDim.x - 32)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + w * 16), "l"(src + (size_t)w * 16)
+                     : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Work items in ticket order; a block holds three tickets: the item it works
+// on, the next (its owner and tile already read, its owner's plan copied to
+// the second plan buffer while the current item runs) and the one after (the
+// atomic claiming it in flight).  Between two items thread 0 alone reads the
+// next owners and tile and releases the finished tile to its instance's copy
+// chunks (fence, then the done counter), the fence overlapping those reads; one
+// barrier on either side.  Holding tickets ahead cannot stall the launch: the
+// smallest ticket held and not yet done is always some block's current item,
+// and an item waits only for smaller tickets.
 template <typename K, int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
 batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst *__restrict__ inst,
-                     const uint32_t *__restrict__ owner, const uint32_t *__restrict__ tloc,
-                     const FixSeg *__restrict__ items,
-                     const uint64_t *__restrict__ citem, BatchTotals tot, Ctrl *ctrl, WaitCfg wc,
-                     unsigned int *flags, unsigned int *done) {
+                     const uint32_t *__restrict__ owner, const uint32_t *__restrict__ tile,
+                     const FixSeg *__restrict__ items, const uint64_t *__restrict__ citem, BatchTotals tot,
+                     Ctrl *ctrl, WaitCfg wc, unsigned int *flags, unsigned int *done) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sm = tile_smem<K>(smem_raw);
-    __shared__ unsigned long long s_ticket;
+    __shared__ __align__(16) unsigned char s_plan[2][sizeof(BatchInst)];
+    __shared__ unsigned long long s_t;  // the current ticket
+    __shared__ uint32_t s_j, s_k;       // its owner and (a tile) its tile
+    __shared__ uint32_t s_nj;           // the owner of the next ticket (kNoInst past the end)
+    __shared__ uint32_t s_held[2];      // the instance whose plan each buffer holds
     __shared__ int s_ok;
-    __shared__ uint32_t s_j, s_local;
-    __shared__ __align__(16) unsigned char s_inst_raw[sizeof(BatchInst)];
     __shared__ TileShared ts;
-    const BatchInst &I = *reinterpret_cast<const BatchInst *>(s_inst_raw);
-    __shared__ uint32_t s_loaded;  // instance whose plan s_inst_raw holds
-    if (threadIdx.x == 0) s_loaded = 0xFFFFFFFFu;
-    TicketPipe tp;
-    for (unsigned long long t = ticket_first(ctrl, &s_ticket); t < tot.tiles + tot.chunks;
-         t = ticket_advance(tp, &s_ticket)) {
-        ticket_claim(ctrl, tp);
+    const uint64_t total = tot.tiles + tot.chunks;
+    unsigned long long t1 = 0, t2 = 0;  // thread 0: the next ticket and the one after
+    if (threadIdx.x == 0) {
+        const unsigned long long t0 = atomicAdd(&ctrl->ticket, 1ull);
+        t1 = atomicAdd(&ctrl->ticket, 1ull);
+        s_t = t0;
+        s_j = t0 < total ? owner[t0] : kNoInst;
+        s_k = t0 < tot.tiles ? tile[t0] : 0;
+        s_nj = t1 < total ? owner[t1] : kNoInst;
+        s_held[0] = s_held[1] = kNoInst;
+    }
+    __syncthreads();
+    while (s_t < total) {
+        const unsigned long long t = s_t;
+        const uint32_t j = s_j, nj = s_nj;
+        if (threadIdx.x == 0) t2 = atomicAdd(&ctrl->ticket, 1ull);  // read after this item
+        int cb = s_held[0] == j ? 0 : s_held[1] == j ? 1 : -1;
+        if (cb < 0) {  // not prefetched (the block's first item): copy it now
+            cb = s_held[0] == nj ? 1 : 0;
+            const uint4 *src = reinterpret_cast<const uint4 *>(inst + j);
+            uint4 *dst = reinterpret_cast<uint4 *>(s_plan[cb]);
+            for (uint32_t w = threadIdx.x; w < kPlanWords; w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            if (threadIdx.x == 0) s_held[cb] = j;  // read again only after the next barrier
+        }
+        const BatchInst &I = *reinterpret_cast<const BatchInst *>(s_plan[cb]);
+        const bool pf = nj != kNoInst && nj != j && s_held[1 - cb] != nj;
+        if (pf) prefetch_plan(inst, nj, s_plan[1 - cb]);
         const bool is_tile = t < tot.tiles;
+        if (is_tile) {
+            btree_stream_tile(I.S, keys + I.off, scr + I.scr_base, flags + I.tile_base, ctrl, wc, s_k, sm, ts);
+        } else {
+            if (threadIdx.x == 0) s_ok = wait_flag(&done[j], (unsigned int)I.S.ntiles, ctrl, wc) ? 1 : 0;
+            __syncthreads();
+            if (s_ok) {
+                const uint64_t c = t - tot.tiles - I.chunk_base;
+                if (I.S.plan == PLAN_O)
+                    batch_copy_items(keys, scr, I, items, citem, c);
+                else
+                    batch_copy_ranges(keys, scr, I, c);
+            }
+            load_tile_wait();  // the plan prefetch, where there is one
+        }
+        __syncthreads();  // the item is done (every store of a tile issued); a prefetched plan has landed
         if (threadIdx.x == 0) {
-            s_j = owner[t];
-            if (is_tile) s_local = tloc[t];
-            s_ok = 1;
-            if (!is_tile) s_ok = wait_flag(&done[s_j], (unsigned int)inst[s_j].S.ntiles, ctrl, wc) ? 1 : 0;
+            const unsigned long long n = t1;
+            const uint32_t k1 = n < tot.tiles ? tile[n] : 0;
+            const uint32_t j2 = t2 < total ? owner[t2] : kNoInst;
+            if (is_tile) {  // the tile's stores, every thread's, before its count
+                __threadfence();
+                atomicAdd(&done[j], 1u);
+            }
+            if (pf) s_held[1 - cb] = nj;
+            s_t = n;
+            s_j = nj;
+            s_k = k1;
+            s_nj = j2;
+            t1 = t2;
         }
         __syncthreads();
-        if (s_j != s_loaded) {  // the owner's plan into shared memory: every thread reads it many times
-            const uint4 *src = reinterpret_cast<const uint4 *>(inst + s_j);
-            uint4 *dst = reinterpret_cast<uint4 *>(s_inst_raw);
-            for (uint32_t w = threadIdx.x; w < sizeof(BatchInst) / 16; w += blockDim.x) dst[w] = src[w];
-            __syncthreads();
-            if (threadIdx.x == 0) s_loaded = s_j;
-        }
-        if (!s_ok) continue;
-        if (is_tile) {
-            const uint64_t k = btree_tile_of_ticket(I.S, s_local);
-            btree_stream_tile(I.S, keys + I.off, scr + I.scr_base, flags + I.tile_base, ctrl, wc, k, sm, ts);
-            __syncthreads();  // every store of the tile issued before it counts as done
-            if (threadIdx.x == 0) {
-                __threadfence();
-                atomicAdd(&done[s_j], 1u);
-            }
-        } else if (I.S.plan == PLAN_O) {
-            batch_copy_items(keys, scr, I, items, citem, t - tot.tiles - I.chunk_base);
-        } else {
-            batch_copy_ranges(keys, scr, I, t - tot.tiles - I.chunk_base);
-        }
     }
 }
 
@@ -634,18 +685,20 @@ static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStr
     rc = interleave_tiles(P, off, own, loc);
     if (rc) return rc;
     if (P.owner) cudaFreeAsync(P.owner, st);
-    if (P.tloc) cudaFreeAsync(P.tloc, st);
-    P.owner = P.tloc = nullptr;
+    if (P.tile) cudaFreeAsync(P.tile, st);
+    P.owner = P.tile = nullptr;
     const uint64_t nowner = P.tot.tiles + P.tot.chunks;
     if (nowner) {
         TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&P.owner), nowner * sizeof(uint32_t), st));
-        TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&P.tloc), std::max<uint64_t>(P.tot.tiles, 1) * sizeof(uint32_t), st));
+        TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&P.tile),
+                                    std::max<uint64_t>(P.tot.tiles, 1) * sizeof(uint32_t), st));
         if (P.tot.tiles) {
             TL_CUDA_TRY(cudaMemcpyAsync(P.owner, own.data(), own.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-            TL_CUDA_TRY(cudaMemcpyAsync(P.tloc, loc.data(), loc.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            TL_CUDA_TRY(cudaMemcpyAsync(P.tile, loc.data(), loc.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         }
-        const unsigned g = (unsigned)std::min<uint64_t>(((uint64_t)P.num * 32 + 255) / 256, (uint64_t)batch_sms() * 8);
-        batch_owner_kernel<<<g, 256, 0, st>>>(P.inst, P.num, P.tot.tiles, P.owner);
+        const uint64_t work = std::max<uint64_t>((uint64_t)P.num * 32, P.tot.tiles);
+        const unsigned g = (unsigned)std::min<uint64_t>((work + 255) / 256, (uint64_t)batch_sms() * 8);
+        batch_owner_kernel<<<g, 256, 0, st>>>(P.inst, P.num, P.tot.tiles, P.owner, P.tile);
         TL_CUDA_TRY(cudaGetLastError());
         TL_CUDA_TRY(cudaStreamSynchronize(st));  // the plan is complete when this returns, for any stream
     }
@@ -676,7 +729,7 @@ int batch_plan_create(const int64_t *dev_offsets, uint32_t num, uint64_t b, uint
     if (rc) {
         cudaFree(P->inst);
         if (P->owner) cudaFree(P->owner);
-        if (P->tloc) cudaFree(P->tloc);
+        if (P->tile) cudaFree(P->tile);
         free_order_buffers(*P);
         delete P;
         return rc;
@@ -690,7 +743,7 @@ int batch_plan_destroy(tl_batch_plan *plan) {
     auto *P = reinterpret_cast<tl_batch_plan_impl *>(plan);
     cudaFree(P->inst);
     if (P->owner) cudaFree(P->owner);
-    if (P->tloc) cudaFree(P->tloc);
+    if (P->tile) cudaFree(P->tile);
     free_order_buffers(*P);
     delete P;
     return TL_SUCCESS;
@@ -733,7 +786,7 @@ static int launch_batch_permute(const tl_batch_plan_impl &P, K *keys, char *ws, 
     const uint64_t work = P.tot.tiles + P.tot.chunks;
     if (work == 0) return TL_SUCCESS;
     const uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * batch_sms(), work);
-    kern<<<(unsigned)grid, threads, smem, st>>>(keys, scr, P.inst, P.owner, P.tloc, P.items, P.citem, P.tot, ctrl, wc,
+    kern<<<(unsigned)grid, threads, smem, st>>>(keys, scr, P.inst, P.owner, P.tile, P.items, P.citem, P.tot, ctrl, wc,
                                                  flags, done);
     TL_CUDA_TRY(cudaGetLastError());
     return TL_SUCCESS;
