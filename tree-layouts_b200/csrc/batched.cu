@@ -235,15 +235,17 @@ __device__ __forceinline__ void prefetch_plan(const BatchInst *inst, uint32_t j,
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-// Work items in ticket order; a block holds three tickets: the item it works
-// on, the next (its owner and tile already read, its owner's plan copied to
-// the second plan buffer while the current item runs) and the one after (the
-// atomic claiming it in flight).  Between two items thread 0 alone reads the
-// next owners and tile and releases the finished tile to its instance's copy
-// chunks (fence, then the done counter), the fence overlapping those reads; one
-// barrier on either side.  Holding tickets ahead cannot stall the launch: the
-// smallest ticket held and not yet done is always some block's current item,
-// and an item waits only for smaller tickets.
+// Work items in ticket order; a block holds four tickets: the item it works
+// on, the next (its owner and tile known, its owner's plan copied to the
+// second plan buffer while the current item runs), the one after (its owner
+// copied to shared memory while the current item runs) and a fourth (the
+// atomic claiming it in flight).  Thread 0 starts those copies (cp.async, no
+// registers held across the item) as an item starts; between two items it
+// alone releases the finished tile to its instance's copy chunks (fence, then
+// the done counter) and moves the pipeline on, one barrier on either side.
+// Holding tickets ahead cannot stall the launch: the smallest ticket held and
+// not yet done is always some block's current item, and an item waits only
+// for smaller tickets.
 template <typename K, int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
 batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst *__restrict__ inst,
@@ -257,13 +259,15 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
     __shared__ uint32_t s_j, s_k;       // its owner and (a tile) its tile
     __shared__ uint32_t s_nj;           // the owner of the next ticket (kNoInst past the end)
     __shared__ uint32_t s_held[2];      // the instance whose plan each buffer holds
+    __shared__ uint32_t s_k1, s_j2;     // the tile of the next ticket, the owner of the one after
     __shared__ int s_ok;
     __shared__ TileShared ts;
     const uint64_t total = tot.tiles + tot.chunks;
-    unsigned long long t1 = 0, t2 = 0;  // thread 0: the next ticket and the one after
+    uint32_t t1 = 0, t2 = 0;  // thread 0: the next ticket and the one after (below 2^31, as built)
     if (threadIdx.x == 0) {
         const unsigned long long t0 = atomicAdd(&ctrl->ticket, 1ull);
-        t1 = atomicAdd(&ctrl->ticket, 1ull);
+        t1 = (uint32_t)atomicAdd(&ctrl->ticket, 1ull);
+        t2 = (uint32_t)atomicAdd(&ctrl->ticket, 1ull);
         s_t = t0;
         s_j = t0 < total ? owner[t0] : kNoInst;
         s_k = t0 < tot.tiles ? tile[t0] : 0;
@@ -274,7 +278,17 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
     while (s_t < total) {
         const unsigned long long t = s_t;
         const uint32_t j = s_j, nj = s_nj;
-        if (threadIdx.x == 0) t2 = atomicAdd(&ctrl->ticket, 1ull);  // read after this item
+        uint32_t t3 = 0;
+        if (threadIdx.x == 0) {  // read as the item ends
+            if (t1 < tot.tiles)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_k1)),
+                             "l"(tile + t1) : "memory");
+            if (t2 < total)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_j2)),
+                             "l"(owner + t2) : "memory");
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            t3 = (uint32_t)atomicAdd(&ctrl->ticket, 1ull);
+        }
         int cb = s_held[0] == j ? 0 : s_held[1] == j ? 1 : -1;
         if (cb < 0) {  // not prefetched (the block's first item): copy it now
             cb = s_held[0] == nj ? 1 : 0;
@@ -305,8 +319,8 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
         __syncthreads();  // the item is done (every store of a tile issued); a prefetched plan has landed
         if (threadIdx.x == 0) {
             const unsigned long long n = t1;
-            const uint32_t k1 = n < tot.tiles ? tile[n] : 0;
-            const uint32_t j2 = t2 < total ? owner[t2] : kNoInst;
+            load_tile_wait();
+            const uint32_t k1 = t1 < tot.tiles ? s_k1 : 0, j2 = t2 < total ? s_j2 : kNoInst;
             if (is_tile) {  // the tile's stores, every thread's, before its count
                 __threadfence();
                 atomicAdd(&done[j], 1u);
@@ -317,6 +331,7 @@ batch_permute_kernel(K *__restrict__ keys, K *__restrict__ scr, const BatchInst 
             s_k = k1;
             s_nj = j2;
             t1 = t2;
+            t2 = t3;
         }
         __syncthreads();
     }
@@ -644,7 +659,8 @@ static int interleave_tiles(const tl_batch_plan_impl &P, const std::vector<int64
         const uint64_t R = (nt[j] + G - 1) / G;
         for (uint64_t r = 0; r < R; ++r) runs.push_back(Run{((double)r + 0.5) / (double)R, j, (uint32_t)r});
     }
-    if (sum != P.tot.tiles || sum >= (1ull << 32)) return TL_ERROR_UNSUPPORTED;
+    // tile indices and the kernel's tickets are 32-bit
+    if (sum != P.tot.tiles || sum + P.tot.chunks >= (1ull << 31)) return TL_ERROR_UNSUPPORTED;
     std::stable_sort(runs.begin(), runs.end(), [](const Run &a, const Run &b) { return a.key < b.key; });
     own.clear();
     loc.clear();
@@ -986,8 +1002,8 @@ int batch_autotune(tl_batch_plan *plan, const int64_t *dev_offsets, void *dev_ke
         best = total / 2;
         return TL_SUCCESS;
     };
-    const uint32_t tiles[3] = {(uint32_t)(8192 / P.key_bytes), (uint32_t)(16384 / P.key_bytes),
-                               (uint32_t)(32768 / P.key_bytes)};
+    const uint32_t tiles[3] = {(uint32_t)(16384 / P.key_bytes), (uint32_t)(32768 / P.key_bytes),
+                               (uint32_t)(65536 / P.key_bytes)};
     float cur = 0.f;
     rc = time_permute(cur);
     // block size
