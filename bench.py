@@ -440,18 +440,23 @@ def run_ours(args, rank, world, local):
         A.copy_(pristine)
         T.permute(layout, A, b or 16)  # the layout again, for the queries below
 
-    # the reference's algorithm family as a variant (BST: involutions), device time
+    # the reference's algorithm family as a variant (BST, B-tree: involutions), device time
     vinfo = None
-    if args.variants and layout == "bst":
+    if args.variants and layout in ("bst", "btree"):
+        perm_ref = A.clone()  # the stream permutation's layout (A holds it here)
         vms = []
-        for i in range(2 + 3):
+        for i in range(1 + 2):
             A.copy_(pristine)  # untimed
-            r = T.permute_algorithm("bst", "involutions", A, 1, timed=True)
-            if i >= 2:
+            r = T.permute_algorithm(layout, "involutions", A, b or 1, timed=True)
+            if i >= 1:
                 vms.append(r)
         v_med = statistics.median(vms)
+        kern = ("bitrev + lowrev swaps (+ 2 involutions and 3 reversals if non-perfect)" if layout == "bst" else
+                "per level: 2 base-(b+1) digit-reversal swap passes + 2 modular involutions "
+                "(+ 4 involutions and 6 reversals for the partial last level)")
         vinfo = {"involutions": {"ms": round(v_med, 4), "GBps": round(bytes_step / (v_med * 1e-3) / 1e9, 1),
-                                 "kernels": "bitrev + lowrev swaps (+ 2 involutions and 3 reversals if non-perfect)"}}
+                                 "kernels": kern, "equal_to_stream": bool(torch.equal(A, perm_ref))}}
+        del perm_ref
         A.copy_(pristine)
         T.permute(layout, A, b or 16)  # the library's layout again, for the queries below
 

@@ -1,7 +1,8 @@
-"""The reference's BST-by-involutions family as a variant of the permutation
-(tl_permute_algorithm), through the C ABI: bit-exact against the oracle at
-sizes it finishes in seconds (perfect and non-perfect trees, both key widths)
-and equal to the library's own stream permutation at larger sizes."""
+"""The reference's involutions family (BST and B-tree) as a variant of the
+permutation (tl_permute_algorithm), through the C ABI: bit-exact against the
+oracle at sizes it finishes in seconds (perfect and non-perfect trees, both key
+widths, leaves with and without full nodes) and equal to the library's own
+stream permutation at larger sizes."""
 import numpy as np
 import pytest
 
@@ -31,4 +32,34 @@ def test_bst_involutions_equal_stream(n):
     a, s = keys.clone(), keys.clone()
     assert T.permute_algorithm("bst", "involutions", a, 1, timed=True) > 0
     T.permute_algorithm("bst", "stream", s, 1)
+    assert torch.equal(a, s)
+
+
+BTREE_SIZES = {
+    2: list(range(1, 120)) + [3**9 - 1, 3**9, 3**9 + 5, 100003],
+    3: list(range(1, 90)) + [4**7 - 1, 4**7 + 2, 70001],
+    8: list(range(1, 100)) + [9**4 - 1, 9**4, 9**5 - 1, 9**5 + 9, 654321],
+    16: [1, 15, 16, 17, 33, 288, 289, 290, 17**3 - 1, 17**3 + 16, 17**4 - 1, 17**4 + 100, 1000003],
+    1: [1, 2, 3, 7, 8, 100, 4095, 4097],
+    33: [5, 33, 34, 100, 1155, 34**3 - 1, 50000],
+}
+
+
+@pytest.mark.parametrize("b", sorted(BTREE_SIZES))
+@pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
+def test_btree_involutions_bit_exact(b, dtype):
+    for n in BTREE_SIZES[b]:
+        keys = data.sorted_keys_np(n, 1, 3, 17 + n, dtype)
+        t = to_dev(keys)
+        T.permute_algorithm("btree", "involutions", t, b)
+        assert np.array_equal(from_dev(t), O.permute("btree", keys, b)), (b, n)
+
+
+@pytest.mark.parametrize("n,b", [(17**6 - 1, 16), (50_000_017, 16), (9**8 - 1, 8), (30_000_001, 8)])
+def test_btree_involutions_equal_stream(n, b):
+    import torch
+    keys = data.sorted_keys_torch(n, 1, 16, 37, 8)
+    a, s = keys.clone(), keys.clone()
+    assert T.permute_algorithm("btree", "involutions", a, b, timed=True) > 0
+    T.permute_algorithm("btree", "stream", s, b)
     assert torch.equal(a, s)

@@ -1,11 +1,12 @@
 // The reference's other algorithm families as selectable variants of the
 // permutation, for ablations and as a second route to the same layouts.
 //
-// Built: the BST by involutions (the reference's bst-involutions family,
-// gpu/src/bst-involutions.cuh:29-195, restating the published method of
-// Berney and Sitchinava): every step is a self-inverse permutation applied by
-// independent swaps, so each is one grid-wide launch with no scratch and no
-// waits.
+// Built: the BST and the B-tree by involutions (the reference's involutions
+// family, gpu/src/bst-involutions.cuh:29-195 and gpu/src/btree-involutions.cuh:
+// 30-168, restating the published method of Berney and Sitchinava): every step
+// is a self-inverse permutation applied by independent swaps, so each is one
+// grid-wide launch with no scratch and no waits.
+// BST:
 //  - perfect tree, n = 2^d - 1, ranks r = i + 1 in [1, 2^d - 1]: swap r with its
 //    d-bit reversal, then with r's bits below its leading one reversed;
 //  - otherwise (L = n - (2^h - 1) keys on the last level, which in sorted order
@@ -14,6 +15,19 @@
 //    2L - 1, after Yang, Ellis, Mamakani and Ruskey, "In-place permuting and
 //    perfect shuffling using involutions"), rotate the array left by L (three
 //    reversals), and lay out the 2^h - 1 front keys as a perfect tree.
+// B-tree, k = b + 1 (btree-involutions.cuh:30-168):
+//  - perfect tree of d levels, n = k^d - 1: per level, gather every k-th key
+//    (the separators) to the front in order: swap rank r = i + 1 with its d
+//    base-k digits reversed, then with its low d - 1 digits reversed (a digit
+//    rotation: keys by their lowest digit, the separators first), then b-way
+//    shuffle the n - n/k non-separators back into order (two modular
+//    involutions on n - n/k - 1); recurse on the n/k separators;
+//  - otherwise (h top levels, numLeaves = n - (k^h - 1) keys below them:
+//    l in full leaves, i = l / b separators between those, r = numLeaves % b
+//    in the partial leaf): k-way unshuffle the first l + i keys (separators
+//    last), rotate them right by i, b-way shuffle the l leaf keys back into
+//    order, rotate A[i, n) right by the k^h - 1 - i remaining internal keys,
+//    and lay out the k^h - 1 front keys as a perfect tree.
 // The stream permutation (permute.cu) is the library's own algorithm and the
 // default; this family trades its single pass for 2-7 full passes.
 #include <algorithm>
@@ -61,6 +75,12 @@ __global__ void __launch_bounds__(kVariantThreads) bst_lowrev_kernel(K *A, uint6
     }
 }
 
+// (a b) mod m, a, b < m < 2^63.
+__device__ __forceinline__ uint64_t mul_mod(uint64_t a, uint64_t b, uint64_t m) {
+    if (((a | b) >> 32) == 0) return a * b % m;
+    return (uint64_t)((unsigned __int128)a * b % m);
+}
+
 // x^-1 mod m for gcd(x, m) = 1 (extended Euclid on signed words; m < 2^63).
 __device__ __forceinline__ uint64_t inverse_mod(uint64_t x, uint64_t m) {
     int64_t a = (int64_t)(x % m), b = (int64_t)m, u = 1, v = 0;
@@ -93,7 +113,7 @@ __global__ void __launch_bounds__(kVariantThreads) involution_kernel(K *A, uint6
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; x < m; x += stride) {
         const uint64_t g = gcd64(x, m), mg = m / g;
-        const uint64_t y = mg > 1 ? g * ((c % mg) * inverse_mod(x / g, mg) % mg) : 0;
+        const uint64_t y = mg > 1 ? g * mul_mod(c % mg, inverse_mod(x / g, mg), mg) : 0;
         if (x < y) swap_keys(A, x, y);
     }
 }
@@ -104,6 +124,25 @@ __global__ void __launch_bounds__(kVariantThreads) reverse_kernel(K *A, uint64_t
     const uint64_t half = (hi - lo) / 2, stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += stride)
         swap_keys(A, lo + i, hi - 1 - i);
+}
+
+// Perfect B-tree level step: rank r = i + 1 (d base-k digits) <-> r with its
+// low `low` digits reversed (kl = k^low).
+template <typename K>
+__global__ void __launch_bounds__(kVariantThreads)
+digit_reverse_kernel(K *A, uint64_t n, FastDiv64 fk, uint32_t low, uint64_t kl) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint64_t x = i + 1, rev = 0;
+        for (uint32_t t = 0; t < low; ++t) {
+            uint64_t q, dg;
+            fk.divmod(x, q, dg);
+            rev = rev * fk.d + dg;
+            x = q;
+        }
+        const uint64_t j = x * kl + rev - 1;
+        if (i < j) swap_keys(A, i, j);
+    }
 }
 
 static unsigned grid_for(uint64_t work) {
@@ -135,11 +174,69 @@ static int bst_involutions(K *A, uint64_t n, cudaStream_t st) {
     return TL_SUCCESS;
 }
 
+// k-way shuffle (the N / k keys of each residue class interleaved back) and
+// its inverse, N a multiple of k: two modular involutions on [1, N - 1).
+template <typename K>
+static void kway_shuffle(K *A, uint64_t N, uint64_t k, bool inverse, cudaStream_t st) {
+    if (N <= 2 || k <= 1) return;
+    const uint64_t c0 = inverse ? k : 1, c1 = inverse ? 1 : k;
+    involution_kernel<K><<<grid_for(N), kVariantThreads, 0, st>>>(A, N - 1, c0);
+    involution_kernel<K><<<grid_for(N), kVariantThreads, 0, st>>>(A, N - 1, c1);
+}
+
+// A[lo, hi) rotated right by s (three reversals).
+template <typename K>
+static void rotate_right(K *A, uint64_t lo, uint64_t hi, uint64_t s, cudaStream_t st) {
+    if (s == 0 || s >= hi - lo) return;
+    reverse_kernel<K><<<grid_for((hi - lo) / 2), kVariantThreads, 0, st>>>(A, lo, hi);
+    reverse_kernel<K><<<grid_for(s / 2), kVariantThreads, 0, st>>>(A, lo, lo + s);
+    reverse_kernel<K><<<grid_for((hi - lo - s) / 2), kVariantThreads, 0, st>>>(A, lo + s, hi);
+}
+
+template <typename K>
+static void btree_perfect_involutions(K *A, uint64_t n, uint64_t b, uint32_t d, cudaStream_t st) {
+    const uint64_t k = b + 1;
+    const FastDiv64 fk(k);
+    while (d > 1) {
+        uint64_t kd1 = 1;  // k^(d-1)
+        for (uint32_t t = 0; t + 1 < d; ++t) kd1 *= k;
+        // all d digits (nothing above them: kl unused), then the low d - 1
+        digit_reverse_kernel<K><<<grid_for(n), kVariantThreads, 0, st>>>(A, n, fk, d, 0);
+        digit_reverse_kernel<K><<<grid_for(n), kVariantThreads, 0, st>>>(A, n, fk, d - 1, kd1);
+        kway_shuffle(A + n / k, kd1 * b, b, false, st);
+        n /= k;
+        --d;
+    }
+}
+
+template <typename K>
+static int btree_involutions(K *A, uint64_t n, uint64_t b, cudaStream_t st) {
+    const uint64_t k = b + 1;
+    uint32_t d = 0;  // levels of the largest perfect tree within n keys
+    uint64_t pw = 1;
+    while (pw <= (n + 1) / k) {
+        pw *= k;
+        ++d;
+    }
+    const uint64_t ni = pw - 1;
+    if (ni != n) {
+        const uint64_t nl = n - ni, l = nl - nl % b, i = l / b;
+        kway_shuffle(A, l + i, k, true, st);
+        rotate_right(A, 0, l + i, i, st);
+        kway_shuffle(A + i, l, b, false, st);
+        rotate_right(A, i, n, ni - i, st);
+    }
+    btree_perfect_involutions(A, ni, b, d, st);
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
 int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                       cudaStream_t st, float *ms) {
     if (algorithm == TL_ALGO_STREAM) return permute(layout, dev_A, n, b, key_bytes, nullptr, 0, st, ms);
     if (algorithm != TL_ALGO_INVOLUTIONS) return TL_ERROR_INVALID_VALUE;
-    if (layout != TL_LAYOUT_BST) return TL_ERROR_UNSUPPORTED;  // the B-tree and vEB families are not built
+    if (layout != TL_LAYOUT_BST && layout != TL_LAYOUT_BTREE) return TL_ERROR_UNSUPPORTED;  // vEB: not built
+    if (layout == TL_LAYOUT_BTREE && (b == 0 || b >= (1ull << 31))) return TL_ERROR_INVALID_VALUE;
     if (key_bytes != 4 && key_bytes != 8) return TL_ERROR_INVALID_VALUE;
     if (n > 0 && !dev_A) return TL_ERROR_INVALID_VALUE;
     if (reinterpret_cast<uintptr_t>(dev_A) % key_bytes) return TL_ERROR_INVALID_VALUE;
@@ -150,8 +247,13 @@ int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64
     }
     EventTimer timer(ms != nullptr, st);
     timer.start();
-    const int rc = key_bytes == 8 ? bst_involutions(static_cast<uint64_t *>(dev_A), n, st)
-                                  : bst_involutions(static_cast<uint32_t *>(dev_A), n, st);
+    int rc;
+    if (layout == TL_LAYOUT_BST)
+        rc = key_bytes == 8 ? bst_involutions(static_cast<uint64_t *>(dev_A), n, st)
+                            : bst_involutions(static_cast<uint32_t *>(dev_A), n, st);
+    else
+        rc = key_bytes == 8 ? btree_involutions(static_cast<uint64_t *>(dev_A), n, b, st)
+                            : btree_involutions(static_cast<uint32_t *>(dev_A), n, b, st);
     timer.stop();
     if (rc) return rc;
     const int rs = sync_and_check(st);
