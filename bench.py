@@ -440,9 +440,9 @@ def run_ours(args, rank, world, local):
         A.copy_(pristine)
         T.permute(layout, A, b or 16)  # the layout again, for the queries below
 
-    # the reference's algorithm family as a variant (BST, B-tree: involutions), device time
+    # the reference's algorithm family as a variant (involutions), device time
     vinfo = None
-    if args.variants and layout in ("bst", "btree"):
+    if args.variants and layout in ("bst", "btree", "mveb"):
         perm_ref = A.clone()  # the stream permutation's layout (A holds it here)
         vms = []
         for i in range(1 + 2):
@@ -451,9 +451,12 @@ def run_ours(args, rank, world, local):
             if i >= 1:
                 vms.append(r)
         v_med = statistics.median(vms)
-        kern = ("bitrev + lowrev swaps (+ 2 involutions and 3 reversals if non-perfect)" if layout == "bst" else
-                "per level: 2 base-(b+1) digit-reversal swap passes + 2 modular involutions "
-                "(+ 4 involutions and 6 reversals for the partial last level)")
+        kern = {"bst": "bitrev + lowrev swaps (+ 2 involutions and 3 reversals if non-perfect)",
+                "btree": "per level: 2 base-(b+1) digit-reversal swap passes + 2 modular involutions "
+                         "(+ 4 involutions and 6 reversals for the partial last level)",
+                "mveb": "per split: a (l+1)-way unshuffle and an l-way shuffle (4 modular involutions), "
+                        "balanced bottoms by 2-digit swaps + 2 involutions per round, rotations "
+                        "for non-perfect trees"}[layout]
         vinfo = {"involutions": {"ms": round(v_med, 4), "GBps": round(bytes_step / (v_med * 1e-3) / 1e9, 1),
                                  "kernels": kern, "equal_to_stream": bool(torch.equal(A, perm_ref))}}
         del perm_ref

@@ -119,10 +119,11 @@ int tl_permute_static_ws(int layout, void *dev_A, uint64_t n, uint64_t b, uint32
 /* The reference's algorithm families as variants of tl_permute (its library
  * ships several for each layout: cycle-leader, involutions, hybrid):
  * TL_ALGO_STREAM is this library's own single-pass stream permutation (what
- * tl_permute runs); TL_ALGO_INVOLUTIONS the BST or the B-tree by involutions
- * (gpu/src/bst-involutions.cuh:168-195 timePermuteBST,
- * gpu/src/btree-involutions.cuh:148-168 timePermuteBtree; b 1 .. 2^31 - 1),
- * for ablations and as a second route to the same layout.  Other (layout,
+ * tl_permute runs); TL_ALGO_INVOLUTIONS the BST, the B-tree or the mvEB by
+ * involutions (gpu/src/bst-involutions.cuh:168-195 timePermuteBST,
+ * gpu/src/btree-involutions.cuh:148-168 timePermuteBtree, b 1 .. 2^31 - 1;
+ * gpu/src/mveb-involutions.cuh:502-523 timePermutevEB), for ablations and as
+ * a second route to the same layout.  Other (layout,
  * algorithm) pairs return TL_ERROR_UNSUPPORTED.  Allocates nothing beyond what tl_permute does;
  * synchronous; ms as for tl_permute. */
 typedef enum { TL_ALGO_STREAM = 0, TL_ALGO_INVOLUTIONS = 1 } tl_algorithm;

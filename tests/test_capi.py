@@ -129,8 +129,7 @@ def test_algorithm_variants_not_built_are_refused_before_device_work():
     lib = T.lib()
     lib.tl_permute_algorithm.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32,
                                          C.c_void_p, C.c_void_p]
-    for layout in (T.LAYOUT_MVEB, T.LAYOUT_VEB):
-        assert lib.tl_permute_algorithm(layout, 1, C.c_void_p(256), 1000, 16, 8, None, None) == T.ERROR_UNSUPPORTED
+    assert lib.tl_permute_algorithm(T.LAYOUT_VEB, 1, C.c_void_p(256), 1000, 16, 8, None, None) == T.ERROR_UNSUPPORTED
     assert lib.tl_permute_algorithm(T.LAYOUT_BST, 7, C.c_void_p(256), 1000, 1, 8, None, None) == T.ERROR_INVALID_VALUE
     # B-tree by involutions: b must be 1 .. 2^31 - 1
     assert lib.tl_permute_algorithm(T.LAYOUT_BTREE, 1, C.c_void_p(256), 1000, 0, 8, None, None) == T.ERROR_INVALID_VALUE

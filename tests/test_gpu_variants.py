@@ -1,4 +1,4 @@
-"""The reference's involutions family (BST and B-tree) as a variant of the
+"""The reference's involutions family (BST, B-tree, mvEB) as a variant of the
 permutation (tl_permute_algorithm), through the C ABI: bit-exact against the
 oracle at sizes it finishes in seconds (perfect and non-perfect trees, both key
 widths, leaves with and without full nodes) and equal to the library's own
@@ -62,4 +62,27 @@ def test_btree_involutions_equal_stream(n, b):
     a, s = keys.clone(), keys.clone()
     assert T.permute_algorithm("btree", "involutions", a, b, timed=True) > 0
     T.permute_algorithm("btree", "stream", s, b)
+    assert torch.equal(a, s)
+
+
+MVEB_SIZES = list(range(1, 300)) + [511, 1023, 1024, 2047, 4095, 4097, 32767, 65535, 65536, 70001, 2**20 - 1,
+                                    1_000_003]
+
+
+@pytest.mark.parametrize("dtype", [np.uint32, np.uint64])
+def test_mveb_involutions_bit_exact(dtype):
+    for n in MVEB_SIZES:
+        keys = data.sorted_keys_np(n, 1, 3, 23 + n, dtype)
+        t = to_dev(keys)
+        T.permute_algorithm("mveb", "involutions", t, 1)
+        assert np.array_equal(from_dev(t), O.permute("mveb", keys, 1)), n
+
+
+@pytest.mark.parametrize("n,kb", [(2**24 - 1, 4), (2**16 * 300 + 7, 4), (30_000_001, 8)])
+def test_mveb_involutions_equal_stream(n, kb):
+    import torch
+    keys = data.sorted_keys_torch(n, 1, 3, 41, kb)
+    a, s = keys.clone(), keys.clone()
+    assert T.permute_algorithm("mveb", "involutions", a, 1, timed=True) > 0
+    T.permute_algorithm("mveb", "stream", s, 1)
     assert torch.equal(a, s)

@@ -106,15 +106,21 @@ __device__ __forceinline__ uint64_t gcd64(uint64_t a, uint64_t b) {
 }
 
 // The involution x -> g * (c * (x/g)^-1 mod m/g), g = gcd(x, m), on the keys
-// [1, m) of an array of m + 1 keys (the two ends stay).  c = 1 then c = 2 is the
-// 2-way perfect shuffle; c = 2 then c = 1 its inverse.
+// [1, m) of each of `parts` arrays of m + 1 keys (the two ends stay), array p
+// starting at A + p * pstride + o (o may be -1: its first key is not touched).
+// c = 1 then c = k is the k-way perfect shuffle; c = k then c = 1 its inverse.
 template <typename K>
-__global__ void __launch_bounds__(kVariantThreads) involution_kernel(K *A, uint64_t m, uint64_t c) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; x < m; x += stride) {
+__global__ void __launch_bounds__(kVariantThreads)
+involution_kernel(K *A, uint64_t parts, uint64_t pstride, int64_t o, uint64_t m, uint64_t c) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x, per = m - 1, work = parts * per;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += stride) {
+        const uint64_t p = w / per, x = w - p * per + 1;
         const uint64_t g = gcd64(x, m), mg = m / g;
         const uint64_t y = mg > 1 ? g * mul_mod(c % mg, inverse_mod(x / g, mg), mg) : 0;
-        if (x < y) swap_keys(A, x, y);
+        if (x < y) {
+            K *a = A + (int64_t)(p * pstride) + o;
+            swap_keys(a, x, y);
+        }
     }
 }
 
@@ -159,8 +165,8 @@ static int bst_involutions(K *A, uint64_t n, cudaStream_t st) {
         d = h;
         const uint64_t L = n - ni;
         if (2 * L > 2) {
-            involution_kernel<K><<<grid_for(2 * L), kVariantThreads, 0, st>>>(A, 2 * L - 1, 2);
-            involution_kernel<K><<<grid_for(2 * L), kVariantThreads, 0, st>>>(A, 2 * L - 1, 1);
+            involution_kernel<K><<<grid_for(2 * L), kVariantThreads, 0, st>>>(A, 1, 0, 0, 2 * L - 1, 2);
+            involution_kernel<K><<<grid_for(2 * L), kVariantThreads, 0, st>>>(A, 1, 0, 0, 2 * L - 1, 1);
         }
         reverse_kernel<K><<<grid_for(L / 2), kVariantThreads, 0, st>>>(A, 0, L);
         reverse_kernel<K><<<grid_for((n - L) / 2), kVariantThreads, 0, st>>>(A, L, n);
@@ -175,13 +181,16 @@ static int bst_involutions(K *A, uint64_t n, cudaStream_t st) {
 }
 
 // k-way shuffle (the N / k keys of each residue class interleaved back) and
-// its inverse, N a multiple of k: two modular involutions on [1, N - 1).
+// its inverse, N a multiple of k: two modular involutions on [1, N - 1).  On
+// `parts` arrays of N keys at A + p * pstride + o (o = -1: an array that
+// starts one key before A, whose first key the involutions never touch).
 template <typename K>
-static void kway_shuffle(K *A, uint64_t N, uint64_t k, bool inverse, cudaStream_t st) {
-    if (N <= 2 || k <= 1) return;
+static void kway_shuffle(K *A, uint64_t N, uint64_t k, bool inverse, cudaStream_t st, uint64_t parts = 1,
+                         uint64_t pstride = 0, int64_t o = 0) {
+    if (N <= 2 || k <= 1 || parts == 0) return;
     const uint64_t c0 = inverse ? k : 1, c1 = inverse ? 1 : k;
-    involution_kernel<K><<<grid_for(N), kVariantThreads, 0, st>>>(A, N - 1, c0);
-    involution_kernel<K><<<grid_for(N), kVariantThreads, 0, st>>>(A, N - 1, c1);
+    involution_kernel<K><<<grid_for(parts * N), kVariantThreads, 0, st>>>(A, parts, pstride, o, N - 1, c0);
+    involution_kernel<K><<<grid_for(parts * N), kVariantThreads, 0, st>>>(A, parts, pstride, o, N - 1, c1);
 }
 
 // A[lo, hi) rotated right by s (three reversals).
@@ -231,11 +240,105 @@ static int btree_involutions(K *A, uint64_t n, uint64_t b, cudaStream_t st) {
     return TL_SUCCESS;
 }
 
+// Balanced mvEB step on each array of m = kk^2 - 1 keys in A[0, total): rank
+// r = i + 1 = x1 kk + x0 <-> x0 kk + x1 (the 2-digit base-kk reversal: the
+// kk - 1 root keys to the front, then the keys by their lowest digit).
+template <typename K>
+__global__ void __launch_bounds__(kVariantThreads) digit_swap_kernel(K *A, uint64_t total, uint64_t m, uint64_t kk) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const uint64_t p = g / m, i = g - p * m, r = i + 1;
+        const uint64_t x1 = r / kk, x0 = r - x1 * kk, j = x0 * kk + x1 - 1;
+        if (i < j) swap_keys(A + p * m, i, j);
+    }
+}
+
+__host__ static bool is_pow2(uint64_t x) { return (x & (x - 1)) == 0; }
+
+// The modified vEB split of a d-level tree: root_d + leaf_d = d, leaf_d the
+// power of two at or above ceil((d - 2) / 2) + 1 (gpu/src/mveb-involutions.cuh:
+// 257-266).
+__host__ static void mveb_split(uint32_t d, uint32_t &root_d, uint32_t &leaf_d) {
+    root_d = (d - 2) / 2 + 1;
+    leaf_d = d - root_d;
+    if (!is_pow2(leaf_d)) {
+        uint32_t p = 1;
+        while (p < leaf_d) p <<= 1;
+        leaf_d = p;
+        root_d = d - leaf_d;
+    }
+}
+
+// Every array of m = 2^d - 1 keys (d a power of two) in A[0, total) into mvEB:
+// per round, each array's sqrt(m + 1) - 1 root keys to its front and its
+// bottoms back into order, then the round on arrays of that size.
+template <typename K>
+static void mveb_balanced(K *A, uint64_t total, uint64_t m, uint32_t d, cudaStream_t st) {
+    while (d > 1 && total) {
+        const uint64_t k = (1ull << (d / 2)) - 1;
+        digit_swap_kernel<K><<<grid_for(total), kVariantThreads, 0, st>>>(A, total, m, k + 1);
+        kway_shuffle(A + k, m - k, k, false, st, total / m, m);
+        m = k;
+        d /= 2;
+    }
+}
+
+// A perfect tree of n = 2^d - 1 keys into mvEB: its root keys (every
+// (l + 1)-th) to the front by a (l + 1)-way unshuffle of the n + 1 keys from
+// A - 1, its bottoms back into order by an l-way shuffle; then the bottoms
+// (balanced) and the root.
+template <typename K>
+static void mveb_perfect(K *A, uint64_t n, uint32_t d, cudaStream_t st) {
+    if (n <= 1) return;
+    if (is_pow2(d)) return mveb_balanced(A, n, n, d, st);
+    uint32_t rd, ld;
+    mveb_split(d, rd, ld);
+    const uint64_t r = (1ull << rd) - 1, l = (1ull << ld) - 1;
+    kway_shuffle(A, n + 1, l + 1, true, st, 1, 0, -1);
+    kway_shuffle(A + r, n - r, l, false, st);
+    mveb_balanced(A + r, n - r, l, ld, st);
+    mveb_perfect(A, r, rd, st);
+}
+
+// Any n (gpu/src/mveb-involutions.cuh:350-497): the root keys between full
+// bottoms to the front (unshuffle, rotation, shuffle), the root keys beyond
+// them after those (rotation); the root and full bottoms as perfect trees, the
+// incomplete bottom at the end recursively.
+template <typename K>
+static void mveb_involutions(K *A, uint64_t n, cudaStream_t st) {
+    if (n <= 1) return;
+    uint32_t d = 0;
+    while (d < 63 && (1ull << d) <= n) ++d;  // bit length
+    if (n == (1ull << d) - 1) return mveb_perfect(A, n, d, st);
+    uint32_t rd, ld;
+    mveb_split(d, rd, ld);
+    const uint64_t r = (1ull << rd) - 1, l = (1ull << ld) - 1;
+    const uint64_t nf = (n - r) / l, inc = n - r - nf * l, tn = nf * (l + 1);
+    kway_shuffle(A, tn, l + 1, true, st);
+    rotate_right(A, 0, tn, nf, st);
+    kway_shuffle(A + nf, tn - nf, l, false, st);
+    if (nf < r) rotate_right(A, nf, n, r - nf, st);
+    if (rd == ld) {
+        mveb_balanced(A, n - inc, r, rd, st);
+    } else {
+        mveb_balanced(A + r, nf * l, l, ld, st);
+        mveb_perfect(A, r, rd, st);
+    }
+    mveb_involutions(A + (n - inc), inc, st);
+}
+
+template <typename K>
+static int mveb_involutions_run(K *A, uint64_t n, cudaStream_t st) {
+    mveb_involutions(A, n, st);
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
 int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                       cudaStream_t st, float *ms) {
     if (algorithm == TL_ALGO_STREAM) return permute(layout, dev_A, n, b, key_bytes, nullptr, 0, st, ms);
     if (algorithm != TL_ALGO_INVOLUTIONS) return TL_ERROR_INVALID_VALUE;
-    if (layout != TL_LAYOUT_BST && layout != TL_LAYOUT_BTREE) return TL_ERROR_UNSUPPORTED;  // vEB: not built
+    if (layout == TL_LAYOUT_VEB) return TL_ERROR_UNSUPPORTED;  // the reference has it on the CPU only
     if (layout == TL_LAYOUT_BTREE && (b == 0 || b >= (1ull << 31))) return TL_ERROR_INVALID_VALUE;
     if (key_bytes != 4 && key_bytes != 8) return TL_ERROR_INVALID_VALUE;
     if (n > 0 && !dev_A) return TL_ERROR_INVALID_VALUE;
@@ -247,13 +350,17 @@ int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64
     }
     EventTimer timer(ms != nullptr, st);
     timer.start();
-    int rc;
-    if (layout == TL_LAYOUT_BST)
+    int rc = TL_SUCCESS;
+    if (layout == TL_LAYOUT_BST) {
         rc = key_bytes == 8 ? bst_involutions(static_cast<uint64_t *>(dev_A), n, st)
                             : bst_involutions(static_cast<uint32_t *>(dev_A), n, st);
-    else
+    } else if (layout == TL_LAYOUT_BTREE) {
         rc = key_bytes == 8 ? btree_involutions(static_cast<uint64_t *>(dev_A), n, b, st)
                             : btree_involutions(static_cast<uint32_t *>(dev_A), n, b, st);
+    } else {
+        rc = key_bytes == 8 ? mveb_involutions_run(static_cast<uint64_t *>(dev_A), n, st)
+                            : mveb_involutions_run(static_cast<uint32_t *>(dev_A), n, st);
+    }
     timer.stop();
     if (rc) return rc;
     const int rs = sync_and_check(st);
