@@ -58,6 +58,38 @@ def peaks():
         return 6650.0, "fallback"
 
 
+L2_BYTES = 126e6  # B200 L2
+
+
+def query_bytes_model(layout, n, b, kb):
+    """Algorithmic HBM bytes of one exact query: the key (w) and the answer (8)
+    plus one node fetch for every level below the L2-resident depth (the
+    largest k whose levels 0..k-1 hold at most half of L2).  A node fetch is
+    ceil(b w / 32) 32-byte sectors for the B-tree, one sector for BST and vEB.
+    Returns (bytes, l2_levels, levels)."""
+    if layout == "btree":
+        k = b + 1
+        h, pw = 0, 1
+        while pw <= (n + 1) // k:  # levels of the largest perfect top tree
+            pw *= k
+            h += 1
+        sizes = [(k ** lv) * b for lv in range(h)]
+        if pw - 1 != n:
+            sizes.append(n - (pw - 1))  # the last level's keys
+        fetch = -(-b * kb // 32) * 32
+    else:
+        d = n.bit_length()
+        sizes = [min(1 << lv, n - ((1 << lv) - 1)) for lv in range(d)]
+        fetch = 32
+    acc, l2_levels = 0, 0
+    for sz in sizes:
+        if acc + sz * kb > L2_BYTES / 2:
+            break
+        acc += sz * kb
+        l2_levels += 1
+    return kb + 8 + fetch * (len(sizes) - l2_levels), l2_levels, len(sizes)
+
+
 def dist_setup(n_gpus):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -480,7 +512,13 @@ def run_ours(args, rank, world, local):
         sans = torch.empty_like(ans)
         T.query("sorted", pristine, Q, sans)
         sms = statistics.median([T.query("sorted", pristine, Q, sans, timed=True) for _ in range(3)])
-        qinfo = {"q": q, "ms": round(qms_med, 3), "queries_per_s": round(q / (qms_med * 1e-3), 1),
+        qbytes, l2lv, nlv = query_bytes_model(layout, n, b or 16, kb)
+        qps = q / (qms_med * 1e-3)
+        qinfo = {"q": q, "ms": round(qms_med, 3), "queries_per_s": round(qps, 1),
+                 "roofline": {"bytes_per_query": qbytes, "levels": nlv, "l2_resident_levels": l2lv,
+                              "roofline_queries_per_s": round(peak * 1e9 / qbytes, 1),
+                              "frac": round(qps * qbytes / (peak * 1e9), 4),
+                              "model": "w + 8 + one node fetch per level below the L2-resident depth"},
                  "hits": hits, "kernel": f"plain {layout} query",
                  "binary_search_queries_per_s": round(q / (sms * 1e-3), 1),
                  "binary_search_hits": int((sans != n).sum().item())}
