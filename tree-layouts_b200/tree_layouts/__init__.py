@@ -192,7 +192,7 @@ ALGORITHMS = {"stream": 0, "involutions": 1}
 
 def permute_algorithm(layout: str, algorithm: str, keys, b: int = 16, stream=None, timed: bool = False):
     """tl_permute_algorithm: the layout by one of the reference's algorithm
-    families ("involutions": BST only) or by this library's own ("stream")."""
+    families ("involutions": BST, B-tree, mvEB) or by this library's own ("stream")."""
     ms = C.c_float(0.0)
     rc = lib().tl_permute_algorithm(LAYOUTS[layout], ALGORITHMS[algorithm], keys.data_ptr(), keys.numel(), b,
                                     _key_bytes(keys), _stream_ptr(stream), C.byref(ms) if timed else None)
