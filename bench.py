@@ -318,13 +318,13 @@ def batched_section(args, dev):
     import tree_layouts.batched as TB
     from tree_layouts import data
 
-    sizes = TB.batch_sizes_np(args.batch_num, 10, 22, 7)
+    sizes = TB.batch_sizes_np(args.batch_num, 10, args.batch_hi, 7)
     keys, off = data.batch_keys_torch(sizes, 64, 7, dev)
     total = int(sizes.sum())
     Q, inst = data.batch_queries_torch(keys, off, args.batch_q, 0.7, 8)
     plan = TB.BatchPlan(off, b=8)
     t0 = time.time()
-    report = plan.autotune(keys, Q, inst)
+    report = plan.autotune(keys, Q, inst) if args.batch_tune else dict(plan.tuning())
     tune_s = time.time() - t0
     pristine = keys.clone()
     ws = plan.workspace()
@@ -362,7 +362,7 @@ def batched_section(args, dev):
     qms = statistics.median(plan.query(keys, Q, inst, ans, timed=True) for _ in range(3))
     del g
     pm = statistics.median(ms)
-    out = {"workload": f"{len(sizes)} uint64 arrays, sizes log-uniform [2^10, 2^22], b = 8, one persistent launch "
+    out = {"workload": f"{len(sizes)} uint64 arrays, sizes log-uniform [2^10, 2^{args.batch_hi}], b = 8, one persistent launch "
                        f"replayed from a CUDA graph; {args.batch_q} queries, 70% hits",
            "arrays": len(sizes), "total_keys": total,
            "permute_ms": round(pm, 3), "permute_GBps": round(2.0 * total * 8 / (pm * 1e-3) / 1e9, 1),
@@ -622,6 +622,8 @@ def main():
     ap.add_argument("--batched", type=int, default=1, help="batched permute/query section (B-tree workloads)")
     ap.add_argument("--batch-num", type=int, default=4096)
     ap.add_argument("--batch-q", type=int, default=2**26)
+    ap.add_argument("--batch-hi", type=int, default=22, help="batched arrays: log2 of the largest size (profiling runs)")
+    ap.add_argument("--batch-tune", type=int, default=1, help="batched: run the autotuner first (0: default tuning)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fixed"],
                     help="B-tree/BST stream schedule: the library's choice, or the fixed-direction ones only")
     args = ap.parse_args()
