@@ -1,11 +1,13 @@
 // The reference's other algorithm families as selectable variants of the
 // permutation, for ablations and as a second route to the same layouts.
 //
-// Built: the BST and the B-tree by involutions (the reference's involutions
-// family, gpu/src/bst-involutions.cuh:29-195 and gpu/src/btree-involutions.cuh:
-// 30-168, restating the published method of Berney and Sitchinava): every step
-// is a self-inverse permutation applied by independent swaps, so each is one
-// grid-wide launch with no scratch and no waits.
+// Built: the BST, the B-tree and the mvEB by involutions (the reference's
+// involutions family, gpu/src/bst-involutions.cuh:29-195,
+// gpu/src/btree-involutions.cuh:30-168 and gpu/src/mveb-involutions.cuh:30-523,
+// restating the published method of Berney and Sitchinava): every step is a
+// self-inverse permutation applied by independent swaps, so each is one
+// grid-wide launch with no scratch and no waits.  (mvEB: see mveb_involutions
+// below.)  Not built: the cycle-leader family and the hybrid BST.
 // BST:
 //  - perfect tree, n = 2^d - 1, ranks r = i + 1 in [1, 2^d - 1]: swap r with its
 //    d-bit reversal, then with r's bits below its leading one reversed;
