@@ -484,14 +484,17 @@ static void free_order_buffers(tl_batch_plan_impl &P) {
     P.ordered = P.ordered_keys = 0;
 }
 
+// A device copy of v, landed when this returns (copied on st, then waited for:
+// a plain cudaMemcpy from pageable memory may return before its DMA lands).
 template <typename T>
-static int upload(T *&dst, const std::vector<T> &v) {
+static int upload(T *&dst, const std::vector<T> &v, cudaStream_t st) {
     if (cudaMalloc(reinterpret_cast<void **>(&dst), std::max<size_t>(v.size(), 1) * sizeof(T)) != cudaSuccess) {
         cudaGetLastError();
         dst = nullptr;
         return TL_ERROR_OUT_OF_MEMORY;
     }
-    if (!v.empty()) TL_CUDA_TRY(cudaMemcpy(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (!v.empty()) TL_CUDA_TRY(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    TL_CUDA_TRY(cudaStreamSynchronize(st));
     return TL_SUCCESS;
 }
 
@@ -519,7 +522,7 @@ static uint64_t order_scratch_keys(const BtreeStream &S, const OrderVectors &v) 
 // threads), its scratch keys listed as copy items and grouped into chunks; then
 // every instance's scratch and chunk bases are recomputed in instance order
 // (the same rules as batch_setup_kernel) and the plan is written back.
-static int order_instances(tl_batch_plan_impl &P, const std::vector<int64_t> &off) {
+static int order_instances(tl_batch_plan_impl &P, const std::vector<int64_t> &off, cudaStream_t st) {
     free_order_buffers(P);
     if (fixed_schedule_only()) return TL_SUCCESS;
     std::vector<uint32_t> cand;
@@ -531,7 +534,8 @@ static int order_instances(tl_batch_plan_impl &P, const std::vector<int64_t> &of
     }
     if (cand.empty()) return TL_SUCCESS;
     std::vector<BatchInst> h(P.num);
-    TL_CUDA_TRY(cudaMemcpy(h.data(), P.inst, h.size() * sizeof(BatchInst), cudaMemcpyDeviceToHost));
+    TL_CUDA_TRY(cudaMemcpyAsync(h.data(), P.inst, h.size() * sizeof(BatchInst), cudaMemcpyDeviceToHost, st));
+    TL_CUDA_TRY(cudaStreamSynchronize(st));
     if (P.b >= 2)  // the host's inverse map (sorted rank of a position) divides by b
         for (uint32_t j : cand) h[j].S.fdb = FastDiv64(P.b);
     std::vector<OrderVectors> ov(cand.size());
@@ -573,7 +577,7 @@ static int order_instances(tl_batch_plan_impl &P, const std::vector<int64_t> &of
         memcpy(tb.data() + toff[i], ov[i].tab.data(), N * sizeof(uint2));
         memcpy(tb.data() + toff[i] + N * sizeof(uint2), ov[i].order.data(), N * sizeof(uint32_t));
     }
-    int rc = upload(P.otab, tb);
+    int rc = upload(P.otab, tb, st);
     if (rc) return rc;
     std::vector<FixSeg> items;
     std::vector<uint64_t> citem;
@@ -623,9 +627,12 @@ static int order_instances(tl_batch_plan_impl &P, const std::vector<int64_t> &of
     }
     P.tot.scratch = bs;
     P.tot.chunks = citem.size();
-    rc = upload(P.items, items);
-    if (!rc) rc = upload(P.citem, citem);
-    if (!rc) TL_CUDA_TRY(cudaMemcpy(P.inst, h.data(), h.size() * sizeof(BatchInst), cudaMemcpyHostToDevice));
+    rc = upload(P.items, items, st);
+    if (!rc) rc = upload(P.citem, citem, st);
+    if (!rc) {
+        TL_CUDA_TRY(cudaMemcpyAsync(P.inst, h.data(), h.size() * sizeof(BatchInst), cudaMemcpyHostToDevice, st));
+        TL_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     if (rc) free_order_buffers(P);
     return rc;
 }
@@ -695,7 +702,7 @@ static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStr
     std::vector<int64_t> off(P.num + 1);
     TL_CUDA_TRY(cudaMemcpyAsync(off.data(), dev_offsets, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     TL_CUDA_TRY(cudaStreamSynchronize(st));
-    int rc = order_instances(P, off);
+    int rc = order_instances(P, off, st);
     if (rc) return rc;
     std::vector<uint32_t> own, loc;
     rc = interleave_tiles(P, off, own, loc);

@@ -229,10 +229,14 @@ bool btree_order_device(const BtreeStream &S, cudaStream_t st, OrderTables &t) {
             cudaGetLastError();
             return false;
         }
-        // synchronous copies from pageable memory: done before the tables are used
-        if ((L && cudaMemcpy(p, e->v.segs.data(), o1, cudaMemcpyHostToDevice) != cudaSuccess) ||
-            cudaMemcpy(p + o1, e->v.tab.data(), N * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(p + o2, e->v.order.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+        // copies on st, then a wait for them: a plain cudaMemcpy from pageable
+        // memory may return before its DMA lands, and a non-blocking stream
+        // would not wait for it
+        if ((L && cudaMemcpyAsync(p, e->v.segs.data(), o1, cudaMemcpyHostToDevice, st) != cudaSuccess) ||
+            cudaMemcpyAsync(p + o1, e->v.tab.data(), N * sizeof(uint2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(p + o2, e->v.order.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
             cudaGetLastError();
             cudaFree(p);
             return false;
