@@ -709,8 +709,12 @@ __device__ __forceinline__ void bar_sync_tail() {
 // lane per level, with their table lookups) and waits for the tiles under
 // their direct parts, so that its work stays off the load's path.  Then the
 // whole block stores the top keys.  Every wait is on a tile with an earlier
-// ticket, and the publish does not depend on warp 0.
-template <typename K>
+// ticket, and the publish does not depend on warp 0.  kRunRegs keeps the
+// current store run in registers across the top-key loop instead of reading it
+// from shared memory for every key (the BST instance: many short runs per
+// tile; measured +3 % there, but not for b = 16, whose kernel keeps the
+// shared-memory reads and its lower register count).
+template <typename K, bool kRunRegs = false>
 __device__ __forceinline__ bool btree_stream_tile(const BtreeStream &S, K *__restrict__ A, K *__restrict__ scr,
                                                   unsigned int *flags, Ctrl *ctrl, const WaitCfg &wc, uint64_t k,
                                                   K *sm, TileShared &ts) {
@@ -786,12 +790,30 @@ __device__ __forceinline__ bool btree_stream_tile(const BtreeStream &S, K *__res
     // top keys, level by level: consecutive threads store consecutive positions
     const uint32_t total = ts.cum[ts.nslots];
     uint32_t r = 0;  // the run of gi only moves forward as gi grows
-    for (uint32_t gi = threadIdx.x; gi < total; gi += blockDim.x) {
-        while (gi >= ts.cum[r + 1]) ++r;
-        const StoreRun run = ts.runs[r];
-        const uint32_t e = gi - ts.cum[r];
-        K *dst = reinterpret_cast<K *>(e < run.nlo ? run.blo : run.bhi);
-        dst[e] = tile[btree_top_item_off(S, run, e)];
+    if constexpr (kRunRegs) {
+        uint32_t c0 = ts.cum[0], c1 = ts.cum[1];
+        StoreRun run = ts.runs[0];
+        for (uint32_t gi = threadIdx.x; gi < total; gi += blockDim.x) {
+            if (gi >= c1) {
+                do {
+                    ++r;
+                } while (gi >= ts.cum[r + 1]);
+                c0 = ts.cum[r];
+                c1 = ts.cum[r + 1];
+                run = ts.runs[r];
+            }
+            const uint32_t e = gi - c0;
+            K *dst = reinterpret_cast<K *>(e < run.nlo ? run.blo : run.bhi);
+            dst[e] = tile[btree_top_item_off(S, run, e)];
+        }
+    } else {
+        for (uint32_t gi = threadIdx.x; gi < total; gi += blockDim.x) {
+            while (gi >= ts.cum[r + 1]) ++r;
+            const StoreRun run = ts.runs[r];
+            const uint32_t e = gi - ts.cum[r];
+            K *dst = reinterpret_cast<K *>(e < run.nlo ? run.blo : run.bhi);
+            dst[e] = tile[btree_top_item_off(S, run, e)];
+        }
     }
     return true;
 }

@@ -48,7 +48,8 @@ constexpr uint64_t stream_tile_keys() {
 
 static inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
-template <typename K>
+// kBst: the instance for b = 1 (see btree_stream_tile's kRunRegs).
+template <typename K, bool kBst = false>
 __global__ void __launch_bounds__(kStreamThreads, kStreamBlocksPerSM)
 btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant__ BtreeStream S, Ctrl *ctrl,
                     WaitCfg wc, unsigned int *flags) {
@@ -59,7 +60,7 @@ btree_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constan
     TicketPipe tp;
     for (unsigned long long t = ticket_first(ctrl, &s_ticket); t < S.ntiles; t = ticket_advance(tp, &s_ticket)) {
         ticket_claim(ctrl, tp);
-        btree_stream_tile(S, A, scr, flags, ctrl, wc, btree_tile_of_ticket(S, t), sm, ts);
+        btree_stream_tile<K, kBst>(S, A, scr, flags, ctrl, wc, btree_tile_of_ticket(S, t), sm, ts);
     }
 }
 
@@ -373,7 +374,7 @@ static int launch_permute_k(const PermutePlan &pl, K *A, char *ws, cudaStream_t 
             TL_CUDA_TRY(cudaGetLastError());
         }
     } else {
-        auto kern = btree_stream_kernel<K>;
+        auto kern = pl.bs.g.b == 1 ? btree_stream_kernel<K, true> : btree_stream_kernel<K, false>;
         TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
