@@ -333,7 +333,7 @@ int tl_debug_struct_size(int which);
 int tl_debug_btree_plan(uint64_t n, uint64_t b);
 /* Schedule tl_permute takes for (layout, n, b, key_bytes) with a workspace of
  * tl_permute_workspace_bytes: 0 right-to-left, 1 left-to-right, 2 ordered
- * tiles (B-tree and BST from 64 tiles up), 3 the vEB engine; < 0 on error. */
+ * tiles (B-tree from 64 tiles up, BST from 16384), 3 the vEB engine; < 0 on error. */
 int tl_debug_permute_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes);
 /* Kernels the last permutation launched (stream pass and second pass). */
 int tl_debug_permute_launches(void);

@@ -249,9 +249,13 @@ struct PermutePlan {
 
 // When a B-tree permutation takes plan O: ORDER_AUTO from kOrderMinTiles tiles
 // up (below that a tile order has too few tiles to pay for its second pass),
-// ORDER_ALWAYS whenever there is a top tree and more than one tile (host replay).
+// for a BST from kOrderMinTilesBst (measured on B200, u64 keys: at 2^20 - 1
+// the fixed schedule takes 34 us against 42, its second pass one launch
+// instead of two; at 2^26 - 1 they tie, 0.289 against 0.290 ms), ORDER_ALWAYS
+// whenever there is a top tree and more than one tile (host replay).
 enum OrderMode { ORDER_NEVER = 0, ORDER_AUTO = 1, ORDER_ALWAYS = 2 };
 constexpr uint64_t kOrderMinTiles = 64;
+constexpr uint64_t kOrderMinTilesBst = 16384;
 // tl_debug_set_schedule: 1 = ORDER_AUTO acts as ORDER_NEVER; 2 = batched plans
 // order every instance that can take the ordered schedule
 static std::atomic<int> g_schedule_mode{0};
@@ -297,7 +301,8 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
         btree_choose_plan(pl.bs, key_bytes);
         if (pl.bs.g.h >= 1 && pl.ntiles >= 2 &&
             (order_mode == ORDER_ALWAYS ||
-             (order_mode == ORDER_AUTO && pl.ntiles >= kOrderMinTiles && !fixed_schedule_only()))) {
+             (order_mode == ORDER_AUTO && pl.ntiles >= (b == 1 ? kOrderMinTilesBst : kOrderMinTiles) &&
+              !fixed_schedule_only()))) {
             if (tables) pl.ot = *tables;
             if (tables || btree_order_host(pl.bs, pl.ot)) {
                 btree_set_ordered(pl.bs, pl.ot.tab, pl.ot.order, pl.ot.scratch_tiles);
