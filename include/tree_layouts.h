@@ -72,13 +72,25 @@ int tl_last_cuda_error(void);
 int tl_layout_position(int layout, uint64_t n, uint64_t b, uint64_t rank, uint64_t *pos);
 
 /* ---------------------------------------------------------------- permutations */
-/* Bytes of device workspace the permutation of (layout, n, b, key_bytes) uses. */
+/* Bytes of device workspace the permutation of (layout, n, b, key_bytes) may
+ * use: enough for the ordered-tile schedule and for the fixed-direction one it
+ * falls back to, so a workspace of this size is always accepted. */
 int tl_permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes,
                                uint64_t *bytes);
 
 /* Generic in-place permutation sorted -> layout.  key_bytes is 4 or 8.
  * dev_workspace may be NULL: the library then allocates it stream-ordered
  * (cudaMallocAsync) and frees it before returning.
+ * Per-geometry tables: a B-tree or BST of 64 tiles or more (16384 for the BST)
+ * takes the ordered-tile schedule, whose tables depend only on (n, b, tile
+ * size).  The first call for a new geometry on a device builds them and copies
+ * them into a cudaMalloc'd block that the library keeps for the life of the
+ * process (at most 64 geometries, about 12 bytes per 32 KB tile plus the fix
+ * segments); that first call therefore allocates and synchronises even when
+ * dev_workspace is given.  If the tables cannot be built or copied (out of
+ * memory, a capturing stream, more than 64 devices or geometries) the call
+ * takes the fixed-direction schedule instead, which the workspace size above
+ * covers.
  * Replaces timePermuteBST (gpu/src/bst-involutions.cuh:168-195),
  * timePermuteBtree (gpu/src/btree-cycles.cuh:77-104) and
  * timePermutevEB (gpu/src/mveb-cycles.cuh:420-440). */
@@ -108,10 +120,12 @@ int tl_permute_veb_std_u64(uint64_t *dev_A, uint64_t n, void *stream, float *ms)
  * compiled into the library, present on every GPU that loads it until the
  * process exits.  It keeps to the fixed-direction schedules (the ordered one
  * needs per-size tables the library would allocate); permutations whose
- * workspace under those exceeds the array return TL_ERROR_UNSUPPORTED.  All calls share that array: calls that overlap
- * on the GPU race, so serialise them.  The first call on a device looks the
- * array up (cudaGetSymbolAddress); make it before any stream capture.
- * Synchronous like tl_permute; allocates nothing. */
+ * workspace under those exceeds the array return TL_ERROR_UNSUPPORTED.  All
+ * calls share that array: calls that overlap on the GPU race, so serialise
+ * them.  The first call on a device looks the array up (cudaGetSymbolAddress);
+ * make it before any stream capture.  Synchronous like tl_permute: it reads
+ * back the status of its device waits and returns after its work on `stream`
+ * has finished.  Allocates nothing. */
 #define TL_STATIC_WORKSPACE_BYTES (32ull << 20)
 int tl_permute_static_ws(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                          void *stream);
@@ -329,7 +343,8 @@ int tl_debug_emulate_unpermute(int layout, uint64_t n, uint64_t b, uint64_t *hos
  * 0 tl_veb_table, 1 tl_rank_model, 2 tl_rank_leaf, 3 tl_rank_train_config. */
 int tl_debug_struct_size(int which);
 /* Fixed-direction schedule of the B-tree permutation for (n, b): 0
- * right-to-left, 1 left-to-right (the one tl_permute_static_ws takes). */
+ * right-to-left, 1 left-to-right (tl_permute_static_ws takes whichever of the
+ * two this returns; tl_permute may take the ordered schedule instead). */
 int tl_debug_btree_plan(uint64_t n, uint64_t b);
 /* Schedule tl_permute takes for (layout, n, b, key_bytes) with a workspace of
  * tl_permute_workspace_bytes: 0 right-to-left, 1 left-to-right, 2 ordered

@@ -13,6 +13,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle as O
 import tree_layouts as T
 from tree_layouts import data
 
@@ -48,6 +49,8 @@ def _static(layout, t, b):
 def test_static_workspace_matches_allocating_entry_point_twice(layout, b, sizes, dtype):
     import torch
     for i, n in enumerate(sizes):  # two calls in a row on the shared array
+        # tl_permute_workspace_bytes covers the fixed-direction schedules this
+        # entry point keeps to, so these sizes fit the static array
         assert T.workspace_bytes(layout, n, b or 16, np.dtype(dtype).itemsize) <= STATIC_BYTES
         keys = data.sorted_keys_np(n, 1, 3 if dtype == np.uint32 else 16, 100 + i, dtype)
         a = _dev(keys)
@@ -56,6 +59,8 @@ def test_static_workspace_matches_allocating_entry_point_twice(layout, b, sizes,
         T.permute(layout, ref, b or 16)
         torch.cuda.synchronize()
         assert torch.equal(a, ref), (layout, n)
+        got = a.cpu().numpy().view(dtype)
+        assert np.array_equal(got, O.permute(layout, keys, b or 16)), (layout, n)
 
 
 def test_static_workspace_refuses_what_does_not_fit():

@@ -681,11 +681,22 @@ static int interleave_tiles(const tl_batch_plan_impl &P, const std::vector<int64
     return TL_SUCCESS;
 }
 
+// Frees a stream-ordered temporary on every exit path.
+struct AsyncBuffer {
+    void *p = nullptr;
+    cudaStream_t st;
+    explicit AsyncBuffer(cudaStream_t s) : st(s) {}
+    ~AsyncBuffer() {
+        if (p) cudaFreeAsync(p, st);
+    }
+};
+
 static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStream_t st) {
-    uint32_t *d_tk = nullptr;
-    BatchTotals *d_tot = nullptr;
-    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_tk), sizeof(P.tile_keys), st));
-    TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_tot), sizeof(BatchTotals), st));
+    AsyncBuffer tk_buf(st), tot_buf(st);
+    TL_CUDA_TRY(cudaMallocAsync(&tk_buf.p, sizeof(P.tile_keys), st));
+    TL_CUDA_TRY(cudaMallocAsync(&tot_buf.p, sizeof(BatchTotals), st));
+    uint32_t *d_tk = static_cast<uint32_t *>(tk_buf.p);
+    BatchTotals *d_tot = static_cast<BatchTotals *>(tot_buf.p);
     TL_CUDA_TRY(cudaMemcpyAsync(d_tk, P.tile_keys, sizeof(P.tile_keys), cudaMemcpyHostToDevice, st));
     batch_setup_kernel<<<1, 256, 0, st>>>(dev_offsets, P.num, P.b, P.key_bytes, FastDiv64(P.b + 1),
                                            FastDiv32((uint32_t)(P.b + 1)),
@@ -696,8 +707,6 @@ static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStr
     TL_CUDA_TRY(cudaMemcpyAsync(&P.tot, d_tot, sizeof(BatchTotals), cudaMemcpyDeviceToHost, st));
     TL_CUDA_TRY(cudaMemcpyAsync(&last, dev_offsets + P.num, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     TL_CUDA_TRY(cudaStreamSynchronize(st));
-    cudaFreeAsync(d_tk, st);
-    cudaFreeAsync(d_tot, st);
     P.total_keys = (uint64_t)last;
     std::vector<int64_t> off(P.num + 1);
     TL_CUDA_TRY(cudaMemcpyAsync(off.data(), dev_offsets, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st));

@@ -437,24 +437,28 @@ int btree_plan_of(uint64_t n, uint64_t b) {
     return pl.bs.plan;
 }
 
+template <typename Kern>
+static int blocks_per_sm_of(Kern kern, size_t smem) {
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem) != cudaSuccess)
+        return -1;
+    return per_sm;
+}
+
+// Resident blocks per SM of the stream kernel instance launch_permute_k picks
+// for the layout (the BST has its own instance), at the 32 KB tile.
 int stream_blocks_per_sm(int layout, uint32_t key_bytes) {
     const size_t smem = 32768 + kTileSmemSlack;
-    int per_sm = 0;
-    cudaError_t e;
+    const bool w8 = key_bytes == 8;
     if (is_veb_layout(layout))
-        e = key_bytes == 8 ? cudaFuncSetAttribute(mveb_stream_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                           : cudaFuncSetAttribute(mveb_stream_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else
-        e = key_bytes == 8 ? cudaFuncSetAttribute(btree_stream_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                           : cudaFuncSetAttribute(btree_stream_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return -1;
-    if (is_veb_layout(layout))
-        e = key_bytes == 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mveb_stream_kernel<uint64_t>, kStreamThreads, smem)
-                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mveb_stream_kernel<uint32_t>, kStreamThreads, smem);
-    else
-        e = key_bytes == 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, btree_stream_kernel<uint64_t>, kStreamThreads, smem)
-                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, btree_stream_kernel<uint32_t>, kStreamThreads, smem);
-    return e == cudaSuccess ? per_sm : -1;
+        return w8 ? blocks_per_sm_of(mveb_stream_kernel<uint64_t>, smem)
+                  : blocks_per_sm_of(mveb_stream_kernel<uint32_t>, smem);
+    if (layout == TL_LAYOUT_BST)
+        return w8 ? blocks_per_sm_of(btree_stream_kernel<uint64_t, true>, smem)
+                  : blocks_per_sm_of(btree_stream_kernel<uint32_t, true>, smem);
+    return w8 ? blocks_per_sm_of(btree_stream_kernel<uint64_t, false>, smem)
+              : blocks_per_sm_of(btree_stream_kernel<uint32_t, false>, smem);
 }
 
 int permute_geometry(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, PermuteGeometry &geo) {
@@ -501,12 +505,18 @@ int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes,
     return TL_SUCCESS;
 }
 
+// Enough for whichever schedule the call ends up on: the ordered schedule when
+// its tables reach the device, else the fixed-direction one (permute() falls
+// back to it when the table upload fails), so a workspace of this size is never
+// refused.
 int permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes) {
     if (!bytes) return TL_ERROR_INVALID_VALUE;
-    PermutePlan pl;
+    PermutePlan pl, fx;
     int rc = make_plan(layout, n, b, key_bytes, pl);
     if (rc) return rc;
-    *bytes = pl.bytes;
+    rc = make_plan(layout, n, b, key_bytes, fx, ORDER_NEVER);
+    if (rc) return rc;
+    *bytes = std::max(pl.bytes, fx.bytes);
     return TL_SUCCESS;
 }
 

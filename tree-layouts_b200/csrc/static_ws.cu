@@ -17,13 +17,15 @@
 //    library would allocate); one whose workspace under them exceeds the array
 //    is rejected with TL_ERROR_UNSUPPORTED before any device work.
 //  - Every call uses the same array and it keeps the previous call's contents.
-//    The permutation clears what must start at zero (the read flags, by a
-//    stream-ordered memset, and the control block, by a copy) on every call.
+//    The permutation clears what must start at zero (the read flags and the
+//    control block behind them, by one stream-ordered memset) on every call.
 //    Calls that overlap on the GPU - on different streams, or from different
 //    host threads without ordering - race on the array; callers serialise them.
 //  - The first call on each device looks the array's device address up with
 //    cudaGetSymbolAddress (once per device, with that device current).  Make
 //    that first call before any stream capture.
+//  - Like tl_permute it is synchronous: it reads the status of its bounded
+//    device waits back and returns after its work on the stream has finished.
 #include <mutex>
 
 #include "internal.h"
