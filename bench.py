@@ -584,6 +584,8 @@ def run_ours(args, rank, world, local):
     roof["traffic"] = measured_traffic(args.workload, n)
     if roof["traffic"] is not None:
         roof["traffic_per_algorithmic_byte"] = round(roof["traffic"] / bytes_step, 4)
+        roof["traffic_source"] = (f"profiles/stream_traffic_{args.workload}.json: ncu dram__bytes_read.sum + "
+                                  "dram__bytes_write.sum of one launch at 2e8 keys, scaled by keys")
 
     # bit-exact check of the last timed permutation against the CPU checker
     # (the reference's own CPU code where it has one), outside the timed region

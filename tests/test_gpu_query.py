@@ -85,3 +85,35 @@ def test_benchmark_query_shapes_small():
     Q = data.queries_np(keys, 200_000, 0.5, 6)
     tree = O.permute("mveb", keys)
     assert np.array_equal(gpu_answers("mveb", tree, Q), O.search("mveb", tree, Q))
+
+
+@pytest.mark.parametrize("layout,b", [("btree", 16), ("btree", 8), ("btree", 2), ("btree", 32), ("btree", 5),
+                                      ("bst", 1), ("mveb", 0)])
+@pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
+def test_queries_on_an_unaligned_layout(layout, b, dtype):
+    """A layout that starts one key past a 16-byte boundary takes the kernels'
+    scalar node reads; answers are unchanged."""
+    import torch
+    for n in [17, 1000, 70001, 1_048_575]:
+        keys = data.sorted_keys_np(n, 1, 16 if dtype == np.uint64 else 3, n + 3, dtype)
+        tree = O.permute(layout, keys, b or 16)
+        Q = data.queries_np(keys, 20_000, 0.5, n + 4)
+        buf = to_dev(np.concatenate([np.zeros(1, dtype), tree]))
+        view = buf[1:]
+        assert view.data_ptr() % 16 != 0
+        ans = torch.empty(len(Q), dtype=torch.int64, device="cuda")
+        T.query(layout, view, to_dev(Q), ans, b or 16)
+        assert np.array_equal(ans.cpu().numpy().view(np.uint64), O.search(layout, tree, Q, b or 16)), (layout, b, n)
+
+
+@pytest.mark.parametrize("b", [1, 2, 3, 4, 5, 7, 8, 9, 15, 16, 17, 31, 32, 33, 64, 100])
+def test_btree_queries_every_node_width(b):
+    """Every node width: 16-byte rows, one key per lane (b <= 32), and the
+    scalar group kernel (b > 32 without 16-byte rows)."""
+    for dtype in (np.uint64, np.uint32):
+        for n in [b, b + 1, 5 * b + 3, 100_003]:
+            keys = data.sorted_keys_np(n, 1, 16 if dtype == np.uint64 else 3, n + b, dtype)
+            tree = O.permute("btree", keys, b)
+            Q = data.queries_np(keys, 10_000, 0.5, b)
+            Q = np.concatenate([Q, keys[:1] - 1 if keys[0] > 0 else keys[:1], keys[-1:] + 1]).astype(dtype)
+            assert np.array_equal(gpu_answers("btree", tree, Q, b), O.search("btree", tree, Q, b)), (b, n, dtype)

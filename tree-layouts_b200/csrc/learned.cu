@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "descent.cuh"
 #include "geometry.cuh"
 #include "internal.h"
 #include "learned.h"
@@ -402,52 +403,36 @@ __device__ __forceinline__ void rank_gaps(const LearnedGeom &G, uint64_t s, uint
     }
 }
 
-template <typename K, int NV>
-__device__ __forceinline__ void node_scan(const K *__restrict__ A, uint64_t n, uint64_t i, K q, uint32_t &lt,
-                                          uint32_t &valid, bool &eq) {
-    constexpr int KPV = 16 / sizeof(K);
-    constexpr int B = NV * KPV;
-    lt = 0;
-    eq = false;
-    if (i + B <= n) {
-        valid = B;
-        const uint4 *node = reinterpret_cast<const uint4 *>(A + i);
-        uint4 v[NV];
-#pragma unroll
-        for (int j = 0; j < NV; ++j) v[j] = __ldg(node + j);
-        const K *all = reinterpret_cast<const K *>(v);
-#pragma unroll
-        for (int j = 0; j < B; ++j) lt += all[j] < q;
-        if (lt < (uint32_t)B) {
-            K at = all[0];
-#pragma unroll
-            for (int j = 1; j < B; ++j)
-                if ((uint32_t)j == lt) at = all[j];
-            eq = at == q;
-        }
-    } else {
-        valid = (uint32_t)(n - i);
-        for (uint32_t j = 0; j < valid; ++j) lt += __ldg(A + i + j) < q;
-        if (lt < valid) eq = __ldg(A + i + lt) == q;
-    }
-}
+// The learned start as a policy of the cooperative descent (descent.cuh).
+// prepare() runs the model for one query per lane and picks the start node;
+// a descent started below the root records whether it saw node keys on either
+// side of the query (flags kSeenLess / kSeenGreater) and, when it falls off the
+// tree without them, restarts from the root.
+constexpr uint32_t kSubtree = 1, kSeenLess = 2, kSeenGreater = 4;
 
-template <typename K, int NV>
-__global__ void __launch_bounds__(256)
-learned_query_kernel(const K *__restrict__ A, const LearnedGeom G, const __grid_constant__ ModelParams p,
-                     int use_net, const tl_rank_leaf *__restrict__ leaves, const K *__restrict__ Q, uint64_t nq,
-                     uint64_t *__restrict__ ans, unsigned long long *__restrict__ stats) {
-    constexpr int B = NV * (16 / sizeof(K));
-    const BtreeGeom &g = G.g;
-    const uint64_t n = g.n;
-    const uint64_t cmax = (n + 1) / (B + 1);
+struct LearnedPolicy {
+    const LearnedGeom &G;
+    const ModelParams &p;
+    const tl_rank_leaf *__restrict__ leaves;
+    int use_net;
     unsigned long long n_fallback = 0, depth_sum = 0;
-    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
-         qi += (uint64_t)gridDim.x * blockDim.x) {
+
+    __device__ LearnedPolicy(const LearnedGeom &g, const ModelParams &pp, const tl_rank_leaf *lv, int un)
+        : G(g), p(pp), leaves(lv), use_net(un) {}
+
+    template <typename K>
+    __device__ __forceinline__ QEntry prepare(const K *__restrict__ Q, uint64_t qi, bool valid) {
+        QEntry e;
+        e.valid = valid;
+        e.node = 0;
+        e.flags = 0;
+        e.key = 0;
+        if (!valid) return e;
+        const BtreeGeom &g = G.g;
+        const uint64_t n = g.n, B = g.b;
         const K q = __ldcs(Q + qi);
-        uint64_t res = n;
-        bool done = false;
-        // 1. predicted rank window -> deepest covering subtree
+        e.key = (uint64_t)q;
+        // predicted rank window -> deepest subtree covering it
         const uint32_t l = leaf_of(p, root_eval(p, feature(p, (uint64_t)q), use_net != 0));
         const tl_rank_leaf lf = leaves[l];
         if (!lf.empty && g.h > 0) {
@@ -468,46 +453,56 @@ learned_query_kernel(const K *__restrict__ A, const LearnedGeom G, const __grid_
                 glo = G.fd.div(glo);
                 --k;
             }
-            depth_sum += k;
-            uint64_t i = g.pw[k] - 1 + glo * B;
-            bool less = false, greater = false;
-            while (i < n) {
-                uint32_t lt, valid;
-                bool eq;
-                node_scan<K, NV>(A, n, i, q, lt, valid, eq);
-                if (eq) {
-                    res = i + lt;
-                    done = true;
-                    break;
-                }
-                less |= lt > 0;
-                greater |= lt < valid;
-                if (i + 1 > cmax) break;
-                i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
-            }
-            if (!done && less && greater) done = true;  // absent: the subtree straddles q
-        }
-        // 2. plain search from the root when the window could not decide
-        if (!done) {
-            ++n_fallback;
-            uint64_t i = 0;
-            while (i < n) {
-                uint32_t lt, valid;
-                bool eq;
-                node_scan<K, NV>(A, n, i, q, lt, valid, eq);
-                if (eq) {
-                    res = i + lt;
-                    break;
-                }
-                if (i + 1 > cmax) break;
-                i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
+            const uint64_t start = g.pw[k] - 1 + glo * B;
+            if (start < n) {
+                depth_sum += k;
+                e.node = start;
+                e.flags = kSubtree;
+                return e;
             }
         }
+        ++n_fallback;  // the plain search from the root
+        return e;
+    }
+    __device__ __forceinline__ uint32_t seen(uint32_t flags, uint32_t lt, uint32_t cnt) const {
+        return flags | (lt > 0 ? kSeenLess : 0u) | (lt < cnt ? kSeenGreater : 0u);
+    }
+    // absent: the subtree held keys on both sides of the query; otherwise the
+    // window could not decide and the search restarts from the root
+    __device__ __forceinline__ bool fell_off(uint64_t &node, uint32_t &flags, bool leader) {
+        if (!(flags & kSubtree) || ((flags & kSeenLess) && (flags & kSeenGreater))) return true;
+        node = 0;
+        flags = 0;
+        if (leader) ++n_fallback;
+        return false;
+    }
+    __device__ __forceinline__ void answer(uint64_t *__restrict__ ans, uint64_t qi, uint64_t res) const {
         __stcs(ans + qi, res);
     }
+};
+
+template <typename K, int G, int QK>
+__global__ void __launch_bounds__(256)
+learned_query_kernel(const K *__restrict__ A, const LearnedGeom LG, const __grid_constant__ ModelParams p,
+                     int use_net, const tl_rank_leaf *__restrict__ leaves, const K *__restrict__ Q, uint64_t nq,
+                     uint64_t *__restrict__ ans, unsigned long long *__restrict__ stats) {
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t per = (nq + warps - 1) / warps;
+    const uint64_t q0 = min(nq, w * per), q1 = min(nq, q0 + per);
+    LearnedPolicy pol(LG, p, leaves, use_net);
+    btree_descend_warp<K, G, 16 / sizeof(K), QK>(A, static_cast<const K *>(nullptr), 0, LG.g.n, LG.g.b, Q, q0, q1, ans,
+                                                 pol);
     if (stats) {
-        atomicAdd(&stats[0], n_fallback);
-        atomicAdd(&stats[1], depth_sum);
+        unsigned long long f = pol.n_fallback, d = pol.depth_sum;
+        for (int o = 16; o > 0; o >>= 1) {
+            f += __shfl_xor_sync(0xFFFFFFFFu, f, o);
+            d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&stats[0], f);
+            atomicAdd(&stats[1], d);
+        }
     }
 }
 
@@ -682,7 +677,9 @@ int query_btree_learned(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank
                         unsigned long long *stats, cudaStream_t st, float *ms) {
     if (!m || !leaves || (q && (!Q || !ans)) || (n && !A)) return TL_ERROR_INVALID_VALUE;
     if (m->n != n) return TL_ERROR_INVALID_VALUE;
-    if (b * 8 % 16 || b * 8 > 256) return TL_ERROR_UNSUPPORTED;  // vector node loads: b in {2,4,8,16,32}
+    // cooperative node loads: b in {2, 4, 8, 16, 32, 64}, 16-byte aligned layout
+    if (b * 8 % 16 || b * 8 > 512 || ((b * 8 / 16) & (b * 8 / 16 - 1))) return TL_ERROR_UNSUPPORTED;
+    if (reinterpret_cast<uintptr_t>(A) & 15) return TL_ERROR_INVALID_VALUE;
     if (q == 0) return TL_SUCCESS;
     LearnedGeom G;
     G.g = make_btree_geom(n, b);
@@ -697,17 +694,18 @@ int query_btree_learned(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank
     auto launch = [&](auto kern) -> int {
         int per_sm = 0;
         TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
-        uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, (q + 255) / 256);
+        uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, (q + 63) / 64);
         kern<<<(unsigned)std::max<uint64_t>(grid, 1), 256, 0, st>>>(A, G, p, use_net, leaves, Q, q, ans, stats);
         return TL_SUCCESS;
     };
     int rc;
     switch (b * 8 / 16) {
-        case 1: rc = launch(learned_query_kernel<uint64_t, 1>); break;
-        case 2: rc = launch(learned_query_kernel<uint64_t, 2>); break;
-        case 4: rc = launch(learned_query_kernel<uint64_t, 4>); break;
-        case 8: rc = launch(learned_query_kernel<uint64_t, 8>); break;
-        case 16: rc = launch(learned_query_kernel<uint64_t, 16>); break;
+        case 1: rc = launch(learned_query_kernel<uint64_t, 1, 2>); break;
+        case 2: rc = launch(learned_query_kernel<uint64_t, 2, 2>); break;
+        case 4: rc = launch(learned_query_kernel<uint64_t, 4, 4>); break;
+        case 8: rc = launch(learned_query_kernel<uint64_t, 8, 4>); break;
+        case 16: rc = launch(learned_query_kernel<uint64_t, 16, 8>); break;
+        case 32: rc = launch(learned_query_kernel<uint64_t, 32, 8>); break;
         default: return TL_ERROR_UNSUPPORTED;
     }
     if (rc) return rc;

@@ -11,6 +11,7 @@
 // the layout the descent visits the same nodes as the reference's searches.
 #include <algorithm>
 
+#include "descent.cuh"
 #include "internal.h"
 #include "tl_common.cuh"
 
@@ -172,64 +173,22 @@ btree_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_t P, 
     }
 }
 
-// One thread per query, for nodes of b*w = 16*NV bytes (node starts are then
-// 16-byte aligned): the node is fetched with NV independent 16-byte loads, so a
-// warp keeps 32 descents in flight.  The last, partially filled leaf (the only
-// node that may cross n) is read with guarded scalar loads.
-template <typename K, int NV>
+// The cooperative descent of descent.cuh: G lanes per node, KPL keys per lane,
+// QK descents in flight per group; contiguous query ranges per warp.  The top
+// levels (whole levels, the first P keys) are pinned in shared memory.
+template <typename K, int G, int KPL, int QK>
 __global__ void __launch_bounds__(kQueryThreads)
-btree_query_vec_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, const K *__restrict__ Q, uint64_t nq,
-                       uint64_t *__restrict__ ans) {
-    constexpr int KPV = 16 / sizeof(K);  // keys per 16-byte vector
-    constexpr int B = NV * KPV;          // == b
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t cmax = (n + 1) / (B + 1);
-    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
-        const K q = __ldcs(Q + qi);
-        uint64_t i = 0, res = n;
-        while (i < n) {
-            uint32_t lt = 0;
-            bool eq = false;
-            if (i + B <= n) {
-                const uint4 *node = reinterpret_cast<const uint4 *>(A + i);
-                uint4 v[NV];
-#pragma unroll
-                for (int j = 0; j < NV; ++j) v[j] = __ldg(node + j);
-#pragma unroll
-                for (int j = 0; j < NV; ++j) {
-                    const K *kk = reinterpret_cast<const K *>(&v[j]);
-#pragma unroll
-                    for (int e = 0; e < KPV; ++e) lt += kk[e] < q;
-                }
-                if (lt < (uint32_t)B) {
-                    const K *all = reinterpret_cast<const K *>(v);
-                    K at = all[0];
-#pragma unroll
-                    for (int j = 1; j < B; ++j)
-                        if ((uint32_t)j == lt) at = all[j];
-                    eq = at == q;
-                }
-            } else {
-                const uint64_t valid = n - i;
-                K at = q;
-                for (uint64_t j = 0; j < valid; ++j) {
-                    const K cur = __ldg(A + i + j);
-                    lt += cur < q;
-                }
-                if (lt < valid) {
-                    at = __ldg(A + i + lt);
-                    eq = at == q;
-                }
-            }
-            if (eq) {
-                res = i + lt;
-                break;
-            }
-            if (i + 1 > cmax) break;
-            i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
-        }
-        __stcs(ans + qi, res);
-    }
+btree_query_coop_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_t P, const K *__restrict__ Q,
+                        uint64_t nq, uint64_t *__restrict__ ans) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *sm = reinterpret_cast<K *>(smem_raw);
+    pin_prefix(A, P, sm);
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t per = (nq + warps - 1) / warps;
+    const uint64_t q0 = min(nq, w * per), q1 = min(nq, q0 + per);
+    PlainPolicy pol;
+    btree_descend_warp<K, G, KPL, QK>(A, sm, P, n, b, Q, q0, q1, ans, pol);
 }
 
 // ---------------------------------------------------------------- mvEB
@@ -239,41 +198,78 @@ btree_query_vec_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, const K 
 // read-only cache.  A descent past the deepest level ends as "absent" (the
 // reference reads past its table there; it only ever issues hits).
 constexpr int kVebThreads = 128;
+constexpr int kVebQueries = 4;                  // descents in flight per thread
+constexpr size_t kVebSmem = 110 * 1024;         // shared memory per block: pos[] + pinned prefix
+constexpr size_t kVebMinPin = 8 * 1024;
 
-template <typename K, typename PosT>
-__device__ __forceinline__ uint64_t veb_descend(const K *__restrict__ A, const K *sm, uint64_t P,
-                                               const tl_veb_table *__restrict__ tab, uint32_t d, K q,
-                                               uint64_t offset, uint64_t limit, PosT *pos, bool &fell) {
+// QK descents per thread in lock-step: every step takes all of a thread's
+// unresolved queries one level down, so their key loads are in flight together
+// and each level's table entry is read once for all of them.  A query leaves
+// the step loop when it finds its key (res), falls off the tree (bit in
+// `fell`: absent) or leaves the division [offset, limit) (neither: the caller
+// tries the next division).  pos[] holds QK columns per thread:
+// pos[(cd * QK + k) * T + tid].
+template <typename K, typename PosT, int QK>
+__device__ __forceinline__ void veb_descend_multi(const K *__restrict__ A, const K *sm, uint64_t P,
+                                                  const tl_veb_table *__restrict__ tab, uint32_t d, const K (&q)[QK],
+                                                  uint64_t offset, uint64_t limit, PosT *pos, uint32_t todo,
+                                                  uint64_t (&res)[QK], uint32_t &fell) {
     const uint32_t T = blockDim.x, tid = threadIdx.x;
+    uint64_t i[QK], index[QK];
+#pragma unroll
+    for (int k = 0; k < QK; ++k) {
+        i[k] = 1;
+        index[k] = 0;
+        pos[k * T + tid] = 1;
+    }
+    uint32_t act = todo;
     uint32_t cd = 0;
-    uint64_t i = 1, index = 0;
-    pos[tid] = 1;
-    fell = false;
-    while (index + offset < limit) {
-        const K cur = key_at(A, sm, P, offset + index);
-        if (q == cur) return offset + index;
-        if (cd + 1 >= d) {
-            fell = true;
-            return ~0ull;
+    while (act) {
+        K cur[QK];
+#pragma unroll
+        for (int k = 0; k < QK; ++k) {
+            cur[k] = K(0);
+            if ((act >> k) & 1u) {
+                if (index[k] + offset < limit)
+                    cur[k] = key_at(A, sm, P, offset + index[k]);
+                else
+                    act &= ~(1u << k);  // left the division: not resolved here
+            }
         }
-        i = 2 * i + (q > cur);
+#pragma unroll
+        for (int k = 0; k < QK; ++k)
+            if (((act >> k) & 1u) && q[k] == cur[k]) {
+                res[k] = offset + index[k];
+                act &= ~(1u << k);
+            }
+        if (!act) break;
+        if (cd + 1 >= d) {
+            fell |= act;
+            break;
+        }
         ++cd;
         const uint64_t L = __ldg(&tab[cd].L), R = __ldg(&tab[cd].R);
         const uint32_t D = __ldg(&tab[cd].D);
         if (D >= cd) {  // not a table built by buildTable: stop instead of reading outside pos[]
-            fell = true;
-            return ~0ull;
+            fell |= act;
+            break;
         }
-        const uint64_t p = (uint64_t)pos[tid + T * D] + R + (i & R) * L;
-        pos[tid + T * cd] = (PosT)p;
-        index = p - 1;
+#pragma unroll
+        for (int k = 0; k < QK; ++k)
+            if ((act >> k) & 1u) {
+                i[k] = 2 * i[k] + (q[k] > cur[k]);
+                const uint64_t p = (uint64_t)pos[(D * QK + k) * T + tid] + R + (i[k] & R) * L;
+                pos[(cd * QK + k) * T + tid] = (PosT)p;
+                index[k] = p - 1;
+            }
     }
-    return ~0ull;
 }
 
 // idx == nullptr: perfect layout, one table (timeQueryvEB); otherwise the
-// non-perfect table set (timeQueryvEB_nonperfect).
-template <typename K, typename PosT>
+// non-perfect table set (timeQueryvEB_nonperfect): the divisions in order, each
+// query until it is resolved.  A block takes QK * T consecutive queries at a
+// time, thread t the queries t, t + T, ...
+template <typename K, typename PosT, int QK>
 __global__ void __launch_bounds__(kVebThreads)
 veb_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, uint32_t dmax,
                  const tl_veb_table *__restrict__ tables, const uint64_t *__restrict__ idx,
@@ -281,33 +277,43 @@ veb_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, uint32_t dmax,
                  uint64_t nq, uint64_t *__restrict__ ans) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PosT *pos = reinterpret_cast<PosT *>(smem_raw);
-    K *sm = reinterpret_cast<K *>(smem_raw + ((size_t)dmax * blockDim.x * sizeof(PosT) + 15) / 16 * 16);
+    K *sm = reinterpret_cast<K *>(smem_raw + ((size_t)dmax * QK * blockDim.x * sizeof(PosT) + 15) / 16 * 16);
     pin_prefix(A, P, sm);
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
-        const K q = __ldcs(Q + qi);
-        uint64_t res = n;
+    const uint64_t T = blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * QK * T; base < nq; base += (uint64_t)gridDim.x * QK * T) {
+        K q[QK];
+        uint64_t res[QK];
+        uint32_t todo = 0, fell = 0;
+#pragma unroll
+        for (int k = 0; k < QK; ++k) {
+            const uint64_t qi = base + k * T + threadIdx.x;
+            res[k] = n;
+            q[k] = K(0);
+            if (qi < nq) {
+                q[k] = __ldcs(Q + qi);
+                todo |= 1u << k;
+            }
+        }
         if (!idx) {
-            bool fell;
-            const uint64_t r = veb_descend<K, PosT>(A, sm, P, tables, bit_length(n), q, 0, n, pos, fell);
-            if (r != ~0ull) res = r;
+            veb_descend_multi<K, PosT, QK>(A, sm, P, tables, bit_length(n), q, 0, n, pos, todo, res, fell);
         } else {
             uint64_t offset = 0;
-            for (uint32_t j = 0; j < num_tables; ++j) {
-                const uint32_t dj = bit_length(n - offset);
+            for (uint32_t j = 0; j < num_tables && todo; ++j) {
                 const uint64_t lim = __ldg(idx + j);
-                bool fell;
-                const uint64_t r = veb_descend<K, PosT>(A, sm, P, tables + __ldg(table_idx + j), dj, q, offset,
-                                                        lim, pos, fell);
-                if (r != ~0ull) {
-                    res = r;
-                    break;
-                }
-                if (fell) break;
+                veb_descend_multi<K, PosT, QK>(A, sm, P, tables + __ldg(table_idx + j), bit_length(n - offset), q,
+                                               offset, lim, pos, todo, res, fell);
+#pragma unroll
+                for (int k = 0; k < QK; ++k)
+                    if (res[k] != n) todo &= ~(1u << k);  // found
+                todo &= ~fell;                             // absent
                 offset = lim;
             }
         }
-        __stcs(ans + qi, res);
+#pragma unroll
+        for (int k = 0; k < QK; ++k) {
+            const uint64_t qi = base + k * T + threadIdx.x;
+            if (qi < nq) __stcs(ans + qi, res[k]);
+        }
     }
 }
 
@@ -369,70 +375,76 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
         }
         P = std::min<uint64_t>(top, a.n);
         size_t smem = P * sizeof(K);
+        // 16-byte rows (b * w = 16 G on an aligned layout), else one key per
+        // lane for b <= 32, else the scalar group kernel below
         const uint64_t node_bytes = a.b * sizeof(K);
-        const int nv = (node_bytes % 16 == 0 && node_bytes <= 256) ? (int)(node_bytes / 16) : 0;
-        if (nv == 1 || nv == 2 || nv == 4 || nv == 8 || nv == 16) {
-            int rc = TL_SUCCESS;
-#define TL_BV(NV)                                                                          \
-    case NV: {                                                                             \
-        auto kern = btree_query_vec_kernel<K, NV>;                                         \
-        rc = persistent_grid(kern, 0, a.q, &grid);                                         \
+        const uint64_t gv = node_bytes % 16 == 0 ? node_bytes / 16 : 0;
+        const bool aligned = (reinterpret_cast<uintptr_t>(A) & 15) == 0;
+        constexpr int KV = 16 / sizeof(K);
+        int rc = TL_SUCCESS;
+        bool done = false;
+#define TL_BC(GG, KK, QK)                                                                  \
+    {                                                                                      \
+        auto kern = btree_query_coop_kernel<K, GG, KK, QK>;                                \
+        rc = persistent_grid(kern, smem, a.q * GG / QK, &grid);                            \
         if (rc) return rc;                                                                 \
-        kern<<<grid, kQueryThreads, 0, st>>>(A, a.n, a.b, Q, a.q, a.answers);              \
-        break;                                                                             \
+        kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, a.b, P, Q, a.q, a.answers);        \
+        done = true;                                                                       \
     }
-            switch (nv) {
-                TL_BV(1)
-                TL_BV(2)
-                TL_BV(4)
-                TL_BV(8)
-                TL_BV(16)
+        if (aligned && (gv == 1 || gv == 2 || gv == 4 || gv == 8 || gv == 16 || gv == 32)) {
+            switch (gv) {
+                case 1: TL_BC(1, KV, 2) break;
+                case 2: TL_BC(2, KV, 2) break;
+                case 4: TL_BC(4, KV, 4) break;
+                case 8: TL_BC(8, KV, 4) break;
+                case 16: TL_BC(16, KV, 8) break;
+                case 32: TL_BC(32, KV, 8) break;
             }
-#undef TL_BV
+        } else if (a.b <= 32) {
+            if (a.b == 1) TL_BC(1, 1, 2)
+            else if (a.b == 2) TL_BC(2, 1, 2)
+            else if (a.b <= 4) TL_BC(4, 1, 4)
+            else if (a.b <= 8) TL_BC(8, 1, 4)
+            else if (a.b <= 16) TL_BC(16, 1, 4)
+            else TL_BC(32, 1, 8)
+        }
+#undef TL_BC
+        if (done) {
             TL_CUDA_TRY(cudaGetLastError());
             return TL_SUCCESS;
         }
-        int G = 1;
-        while (G < 32 && (uint64_t)G < a.b) G <<= 1;
-        int rc = TL_SUCCESS;
-#define TL_BT(GG)                                                                          \
-    case GG: {                                                                             \
-        auto kern = btree_query_kernel<K, GG>;                                             \
-        rc = persistent_grid(kern, smem, a.q * GG, &grid);                                 \
-        if (rc) return rc;                                                                 \
-        kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, a.b, P, Q, a.q, a.answers);        \
-        break;                                                                             \
-    }
-        switch (G) {
-            TL_BT(1)
-            TL_BT(2)
-            TL_BT(4)
-            TL_BT(8)
-            TL_BT(16)
-            TL_BT(32)
+        {  // b > 32 without 16-byte rows: 32 lanes, several slots per lane
+            auto kern = btree_query_kernel<K, 32>;
+            rc = persistent_grid(kern, smem, a.q * 32, &grid);
+            if (rc) return rc;
+            kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, a.b, P, Q, a.q, a.answers);
         }
-#undef TL_BT
     } else {
         const uint32_t dmax = bit_length(a.n);
         if (dmax > 63) return TL_ERROR_UNSUPPORTED;
         const bool np = a.layout == Q_VEB_NP;
         const bool narrow = a.n < (1ull << 32);
-        const size_t pos_bytes = (size_t)dmax * kVebThreads * (narrow ? 4 : 8);
-        P = std::min<uint64_t>(a.n, (kPinBytes - std::min<size_t>(pos_bytes, kPinBytes / 2)) / sizeof(K));
+        // kVebQueries columns of pos[] per thread; the layout's first positions
+        // pinned in what is left of kVebSmem (two blocks per SM)
+        const size_t pos_bytes = (size_t)dmax * kVebQueries * kVebThreads * (narrow ? 4 : 8);
+        const size_t pin_budget = pos_bytes + kVebMinPin <= kVebSmem ? kVebSmem - pos_bytes : kVebMinPin;
+        P = std::min<uint64_t>(a.n, pin_budget / sizeof(K));
         const size_t smem = (pos_bytes + 15) / 16 * 16 + P * sizeof(K);
+        if (smem > 227 * 1024) return TL_ERROR_UNSUPPORTED;  // pos[] of a tree deeper than about 50 levels
         auto launch = [&](auto kern) -> int {
             TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int per_sm = 0;
             TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kVebThreads, smem));
             uint64_t g = (uint64_t)std::max(per_sm, 1) * query_sm_count();
-            uint64_t need = (a.q + kVebThreads - 1) / kVebThreads;
+            uint64_t need = (a.q + kVebQueries * kVebThreads - 1) / (kVebQueries * kVebThreads);
             unsigned gr = (unsigned)std::max<uint64_t>(1, std::min(g, need));
             kern<<<gr, kVebThreads, smem, st>>>(A, a.n, P, dmax, a.tables, np ? a.idx : nullptr,
                                                 np ? a.table_idx : nullptr, np ? a.num_tables : 1u, Q, a.q,
                                                 a.answers);
             return TL_SUCCESS;
         };
-        int rc = narrow ? launch(veb_query_kernel<K, uint32_t>) : launch(veb_query_kernel<K, uint64_t>);
+        int rc = narrow ? launch(veb_query_kernel<K, uint32_t, kVebQueries>)
+                        : launch(veb_query_kernel<K, uint64_t, kVebQueries>);
         if (rc) return rc;
     }
     TL_CUDA_TRY(cudaGetLastError());
