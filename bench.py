@@ -542,6 +542,8 @@ def run_ours(args, rank, world, local):
         n = args.n
     L = T.lib()
     L.tl_debug_set_schedule(1 if args.schedule == "fixed" else 0)
+    L.tl_debug_set_query_variant.argtypes = [CT.c_int]
+    L.tl_debug_set_query_variant(args.query_variant)
     L.tl_debug_permute_phases.argtypes = [CT.c_int, CT.c_void_p, CT.c_uint64, CT.c_uint64, CT.c_uint32,
                                           CT.c_void_p, CT.POINTER(CT.c_float)]
     dev = torch.device("cuda", local)
@@ -618,25 +620,34 @@ def run_ours(args, rank, world, local):
         A.copy_(pristine)
         T.permute(layout, A, b or 16)  # the layout again, for the queries below
 
-    # the reference's algorithm family as a variant (involutions), device time
+    # the reference's algorithm families as variants (involutions, cycle-leader,
+    # hybrid), device time, each checked against the stream permutation's layout
     vinfo = None
     if args.variants and layout in ("bst", "btree", "mveb"):
         perm_ref = A.clone()  # the stream permutation's layout (A holds it here)
-        vms = []
-        for i in range(1 + 2):
-            A.copy_(pristine)  # untimed
-            r = T.permute_algorithm(layout, "involutions", A, b or 1, timed=True)
-            if i >= 1:
-                vms.append(r)
-        v_med = statistics.median(vms)
-        kern = {"bst": "bitrev + lowrev swaps (+ 2 involutions and 3 reversals if non-perfect)",
-                "btree": "per level: 2 base-(b+1) digit-reversal swap passes + 2 modular involutions "
-                         "(+ 4 involutions and 6 reversals for the partial last level)",
-                "mveb": "per split: a (l+1)-way unshuffle and an l-way shuffle (4 modular involutions), "
-                        "balanced bottoms by 2-digit swaps + 2 involutions per round, rotations "
-                        "for non-perfect trees"}[layout]
-        vinfo = {"involutions": {"ms": round(v_med, 4), "GBps": round(bytes_step / (v_med * 1e-3) / 1e9, 1),
-                                 "kernels": kern, "equal_to_stream": bool(torch.equal(A, perm_ref))}}
+        kern = {("bst", "involutions"): "bitrev + lowrev swaps (+ 2 involutions and 3 reversals if non-perfect)",
+                ("btree", "involutions"): "per level: 2 base-(b+1) digit-reversal swap passes + 2 modular "
+                                          "involutions (+ 4 involutions and 6 reversals for the partial last level)",
+                ("mveb", "involutions"): "per split: a (l+1)-way unshuffle and an l-way shuffle (4 modular "
+                                         "involutions), balanced bottoms by 2-digit swaps + 2 involutions per round, "
+                                         "rotations for non-perfect trees",
+                ("bst", "cycles"): "the B-tree cycle-leader steps with b = 1",
+                ("btree", "cycles"): "per round: equidistant gathers (cycle-leader walks + two reversal passes) over "
+                                     "partitions of (b+1)^2 c keys; the partial last level first",
+                ("mveb", "cycles"): "root gathers, rotations, balanced bottoms by rounds of partition gathers",
+                ("bst", "hybrid"): "last level by cycle-leader gathers, perfect part by 2 involutions"}
+        algos = ["involutions", "cycles"] + (["hybrid"] if layout == "bst" else [])
+        vinfo = {}
+        for algo in algos:
+            vms = []
+            for i in range(1 + 2):
+                A.copy_(pristine)  # untimed
+                r = T.permute_algorithm(layout, algo, A, b or 1, timed=True)
+                if i >= 1:
+                    vms.append(r)
+            v_med = statistics.median(vms)
+            vinfo[algo] = {"ms": round(v_med, 4), "GBps": round(bytes_step / (v_med * 1e-3) / 1e9, 1),
+                           "kernels": kern[(layout, algo)], "equal_to_stream": bool(torch.equal(A, perm_ref))}
         del perm_ref
         A.copy_(pristine)
         T.permute(layout, A, b or 16)  # the library's layout again, for the queries below
@@ -755,7 +766,8 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override n (profiling runs)")
     ap.add_argument("--queries", type=int, default=1)
     ap.add_argument("--reverse", type=int, default=1, help="reverse permutation (layout -> sorted) section")
-    ap.add_argument("--variants", type=int, default=1, help="the reference's algorithm family as a variant (BST)")
+    ap.add_argument("--variants", type=int, default=1,
+                    help="the reference's algorithm families as variants (involutions, cycle-leader, hybrid BST)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=50_000_000)
     ap.add_argument("--ref-n", type=int, default=0, help="reference arm keys (0: the workload's full n)")
@@ -771,6 +783,8 @@ def main():
     ap.add_argument("--parity", type=int, default=1, help="bit-exact check against the CPU checker (untimed)")
     ap.add_argument("--layouts", type=int, default=1,
                     help="every layout at 2^30-class sizes, timed and checked (default workload only)")
+    ap.add_argument("--query-variant", type=int, default=0,
+                    help="query kernel variant for measurements (tl_debug_set_query_variant; 0: the default)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fixed"],
                     help="B-tree/BST stream schedule: the library's choice, or the fixed-direction ones only")
     args = ap.parse_args()

@@ -131,16 +131,24 @@ int tl_permute_static_ws(int layout, void *dev_A, uint64_t n, uint64_t b, uint32
                          void *stream);
 
 /* The reference's algorithm families as variants of tl_permute (its library
- * ships several for each layout: cycle-leader, involutions, hybrid):
- * TL_ALGO_STREAM is this library's own single-pass stream permutation (what
- * tl_permute runs); TL_ALGO_INVOLUTIONS the BST, the B-tree or the mvEB by
- * involutions (gpu/src/bst-involutions.cuh:168-195 timePermuteBST,
- * gpu/src/btree-involutions.cuh:148-168 timePermuteBtree, b 1 .. 2^31 - 1;
- * gpu/src/mveb-involutions.cuh:502-523 timePermutevEB), for ablations and as
- * a second route to the same layout.  Other (layout,
- * algorithm) pairs return TL_ERROR_UNSUPPORTED.  Allocates nothing beyond what tl_permute does;
- * synchronous; ms as for tl_permute. */
-typedef enum { TL_ALGO_STREAM = 0, TL_ALGO_INVOLUTIONS = 1 } tl_algorithm;
+ * ships several for each layout: cycle-leader, involutions, hybrid), for
+ * ablations and as other routes to the same layout:
+ *  - TL_ALGO_STREAM: this library's own single-pass stream permutation (what
+ *    tl_permute runs);
+ *  - TL_ALGO_INVOLUTIONS: the BST, the B-tree or the mvEB by involutions
+ *    (gpu/src/bst-involutions.cuh:168-195 timePermuteBST,
+ *    gpu/src/btree-involutions.cuh:148-168 timePermuteBtree, b 1 .. 2^31 - 1;
+ *    gpu/src/mveb-involutions.cuh:502-523 timePermutevEB);
+ *  - TL_ALGO_CYCLES: the B-tree (b 1 .. 2^20 - 1), the BST (the B-tree with
+ *    b = 1) or the mvEB by the cycle-leader family, equidistant gathers and
+ *    rotations (gpu/src/btree-cycles.cuh:77-104 timePermuteBtree,
+ *    gpu/test/build-bst-cycles.cu:39, gpu/src/mveb-cycles.cuh:420-440
+ *    timePermutevEB);
+ *  - TL_ALGO_HYBRID: the BST's last level by cycles and its perfect part by
+ *    involutions (gpu/src/bst-hybrid.cuh:121-148 timePermuteBST).
+ * Other (layout, algorithm) pairs return TL_ERROR_UNSUPPORTED.  Allocates
+ * nothing beyond what tl_permute does; synchronous; ms as for tl_permute. */
+typedef enum { TL_ALGO_STREAM = 0, TL_ALGO_INVOLUTIONS = 1, TL_ALGO_CYCLES = 2, TL_ALGO_HYBRID = 3 } tl_algorithm;
 int tl_permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                          void *stream, float *ms);
 
@@ -310,6 +318,11 @@ typedef struct tl_rank_train_config {
  * dev_leaves holds num_leaves entries. */
 int tl_rank_model_train(const uint64_t *dev_sorted_keys, uint64_t n, const tl_rank_train_config *cfg,
                         tl_rank_model *model, tl_rank_leaf *dev_leaves, void *stream);
+/* Test hook (host only): the root network's output at x[0 .. count) as the
+ * inference kernels compute it, from the network compiled into its exact
+ * piecewise-linear form; *pieces = the number of linear pieces. */
+int tl_debug_rank_model_root(const tl_rank_model *model, const float *x, uint32_t count, float *out,
+                             uint32_t *pieces);
 /* Inference: dev_rank[i] = predicted rank of dev_keys[i]; dev_eps[i] (optional) =
  * max(eps_lo, eps_hi) of its segment (UINT32_MAX for an empty segment). */
 int tl_rank_model_predict(const tl_rank_model *model, const tl_rank_leaf *dev_leaves,
@@ -337,6 +350,12 @@ int tl_debug_set_wait(unsigned int spin_limit, int force_timeout);
  * protocol breaches (stale read, unguarded store, bad wait, position or scratch
  * slot not written exactly once). */
 int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations);
+/* Host replay of tl_permute_algorithm's step list for TL_ALGO_CYCLES or
+ * TL_ALGO_HYBRID on n 64-bit words (test hook): the cycle-leader steps, and
+ * for the hybrid the perfect front part's involutions as a host permutation;
+ * *steps = the number of gather and rotation steps. */
+int tl_debug_emulate_algorithm(int layout, int algorithm, uint64_t n, uint64_t b, uint64_t *host_A,
+                               uint64_t *steps);
 /* Host replay of tl_unpermute's gather on n 64-bit words (test hook). */
 int tl_debug_emulate_unpermute(int layout, uint64_t n, uint64_t b, uint64_t *host_A);
 /* sizeof of the ABI structs, for bindings to check their mirrors:
@@ -359,6 +378,10 @@ int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes);
  * mode 2: batched plans built from then on put every instance the ordered
  * schedule applies to on it, whatever it saves; 0 restores the default. */
 int tl_debug_set_schedule(int mode);
+/* Measurement hook, query kernels: 0 the default; 2 B-tree nodes in 16-byte
+ * loads instead of 32-byte ones; 3 / 4 vEB two / four descents per thread in
+ * lock-step; 5 B-tree top levels pinned in shared memory. */
+void tl_debug_set_query_variant(int v);
 /* Instances of a batched plan on the ordered-tile schedule and their keys: by
  * default those of 64 tiles or more (at the plan's tile size for their size
  * class) whose scratch keys it cuts to 30 % or less. */

@@ -1,8 +1,9 @@
-"""The reference's involutions family (BST, B-tree, mvEB) as a variant of the
-permutation (tl_permute_algorithm), through the C ABI: bit-exact against the
-oracle at sizes it finishes in seconds (perfect and non-perfect trees, both key
-widths, leaves with and without full nodes) and equal to the library's own
-stream permutation at larger sizes."""
+"""The reference's involutions and cycle-leader families (BST, B-tree, mvEB)
+and its hybrid BST as variants of the permutation (tl_permute_algorithm),
+through the C ABI: bit-exact against the oracle at sizes it finishes in
+seconds (perfect and non-perfect trees, both key widths, leaves with and
+without full nodes) and equal to the library's own stream permutation at
+larger sizes."""
 import numpy as np
 import pytest
 
@@ -86,3 +87,56 @@ def test_mveb_involutions_equal_stream(n, kb):
     assert T.permute_algorithm("mveb", "involutions", a, 1, timed=True) > 0
     T.permute_algorithm("mveb", "stream", s, 1)
     assert torch.equal(a, s)
+
+
+CYCLE_CASES = [("btree", b) for b in sorted(BTREE_SIZES)] + [("bst", 1), ("mveb", 0)]
+
+
+def _cycle_sizes(layout, b):
+    if layout == "btree":
+        return BTREE_SIZES[b]
+    if layout == "bst":
+        return SIZES
+    return MVEB_SIZES
+
+
+@pytest.mark.parametrize("layout,b", CYCLE_CASES)
+@pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
+def test_cycles_bit_exact(layout, b, dtype):
+    for n in _cycle_sizes(layout, b):
+        keys = data.sorted_keys_np(n, 1, 3, 19 + n, dtype)
+        t = to_dev(keys)
+        T.permute_algorithm(layout, "cycles", t, b or 1)
+        assert np.array_equal(from_dev(t), O.permute(layout, keys, b or 16)), (layout, b, n)
+
+
+@pytest.mark.parametrize("dtype", [np.uint64, np.uint32])
+def test_hybrid_bst_bit_exact(dtype):
+    for n in SIZES:
+        keys = data.sorted_keys_np(n, 1, 3, 43 + n, dtype)
+        t = to_dev(keys)
+        T.permute_algorithm("bst", "hybrid", t, 1)
+        assert np.array_equal(from_dev(t), O.permute("bst", keys, 1)), n
+
+
+@pytest.mark.parametrize("layout,algo,n,b,kb", [
+    ("btree", "cycles", 17**6 - 1, 16, 8), ("btree", "cycles", 30_000_001, 16, 8), ("btree", "cycles", 9**7 + 3, 8, 4),
+    ("bst", "cycles", 2**24 - 1, 1, 8), ("bst", "cycles", 20_000_003, 1, 4), ("bst", "hybrid", 2**24 - 1, 1, 8),
+    ("bst", "hybrid", 20_000_003, 1, 8), ("mveb", "cycles", 2**24 - 1, 0, 4), ("mveb", "cycles", 30_000_001, 0, 4),
+])
+def test_cycles_equal_stream(layout, algo, n, b, kb):
+    import torch
+    keys = data.sorted_keys_torch(n, 1, 3, 47, kb)
+    a, s = keys.clone(), keys.clone()
+    assert T.permute_algorithm(layout, algo, a, b or 1, timed=True) > 0
+    T.permute_algorithm(layout, "stream", s, b or 16)
+    assert torch.equal(a, s)
+
+
+def test_variants_refuse_what_they_do_not_build():
+    import torch
+    t = torch.zeros(100, dtype=torch.int64, device="cuda")
+    for layout, algo in [("veb", "cycles"), ("btree", "hybrid"), ("mveb", "hybrid"), ("veb", "involutions")]:
+        with pytest.raises(T.TreeLayoutError) as e:
+            T.permute_algorithm(layout, algo, t, 4)
+        assert e.value.status == T.ERROR_UNSUPPORTED

@@ -26,7 +26,6 @@
 #include "batched.h"
 #include "btree_order.h"
 #include "btree_plan.cuh"
-#include "descent.cuh"
 #include "internal.h"
 
 namespace tl {
@@ -435,71 +434,53 @@ batch_query_kernel(const K *__restrict__ keys, const BatchInst *__restrict__ ins
             const K qv = sq[i];
             uint64_t node = 0, res = n;
             const uint64_t cmax = (n + 1) / (b + 1);
+            // node rows in 32-byte (or 16-byte) loads where the instance's keys
+            // and its nodes start on such a boundary, else key by key
+            const uintptr_t abase = reinterpret_cast<uintptr_t>(A);
+            const uint32_t vb = (abase & 31) == 0 && (b * sizeof(K)) % 32 == 0   ? 32u
+                                : (abase & 15) == 0 && (b * sizeof(K)) % 16 == 0 ? 16u
+                                                                                  : 0u;
             while (node < n) {
                 const uint64_t valid = min(b, n - node);
                 uint32_t lt = 0;
-                for (uint64_t s = 0; s < valid; ++s) {
-                    const uint64_t p = node + s;
-                    const K cur = p < PP ? sm[p] : __ldg(A + p);
-                    lt += cur < qv;
-                }
-                if (lt < valid) {
-                    const uint64_t p = node + lt;
-                    const K at = p < PP ? sm[p] : __ldg(A + p);
-                    if (at == qv) {
-                        res = p;
-                        break;
+                bool eq = false;
+                if (vb && valid == b && node >= PP) {
+                    const uint32_t kpl = vb / sizeof(K), nl = (uint32_t)(b / kpl);
+#pragma unroll 4
+                    for (uint32_t j = 0; j < nl; ++j) {
+                        K v[32 / sizeof(K)];
+                        if (vb == 32) {
+                            ldg32(A + node + (uint64_t)j * kpl, v);
+                        } else {
+                            const uint4 x = __ldg(reinterpret_cast<const uint4 *>(A + node + (uint64_t)j * kpl));
+                            const K *kx = reinterpret_cast<const K *>(&x);
+#pragma unroll
+                            for (int e = 0; e < (int)(16 / sizeof(K)); ++e) v[e] = kx[e];
+                        }
+#pragma unroll
+                        for (int e = 0; e < (int)(32 / sizeof(K)); ++e)
+                            if (vb == 32 || e < (int)(16 / sizeof(K))) {
+                                lt += v[e] < qv;
+                                eq |= v[e] == qv;
+                            }
                     }
+                } else {
+                    for (uint64_t s = 0; s < valid; ++s) {
+                        const uint64_t p = node + s;
+                        const K cur = p < PP ? sm[p] : __ldg(A + p);
+                        lt += cur < qv;
+                        eq |= cur == qv;
+                    }
+                }
+                if (eq) {  // keys are unique: the equal key sits at slot lt
+                    res = node + lt;
+                    break;
                 }
                 if (node + 1 > cmax) break;
                 node = (node + 1) * (b + 1) + (uint64_t)lt * b - 1;
             }
             ans[sidx[i]] = res;
         }
-    }
-}
-
-// The cooperative descent (descent.cuh) over the instance-sorted queries: each
-// warp takes a contiguous range of them and walks it run by run (a run = the
-// queries of one instance), with 16-byte node rows where the instance's keys
-// start on a 16-byte boundary (GV lanes per node; GV = 0: never) and one key
-// per lane otherwise (GS lanes per node).  Answers go to the queries' original
-// positions.
-struct BatchAnswerPolicy : PlainPolicy {
-    const uint64_t *__restrict__ sidx;
-    __device__ explicit BatchAnswerPolicy(const uint64_t *s) : sidx(s) {}
-    __device__ __forceinline__ void answer(uint64_t *__restrict__ ans, uint64_t qi, uint64_t res) const {
-        ans[__ldg(sidx + qi)] = res;
-    }
-};
-
-template <typename K, int GV, int GS, int QK>
-__global__ void __launch_bounds__(kBatchThreads)
-batch_query_coop_kernel(const K *__restrict__ keys, const BatchInst *__restrict__ inst, const K *__restrict__ sq,
-                        const uint32_t *__restrict__ sinst, const uint64_t *__restrict__ sidx,
-                        const unsigned long long *__restrict__ bend, const unsigned long long *__restrict__ nvalid,
-                        uint64_t *__restrict__ ans) {
-    const uint64_t q = *nvalid;  // queries with a valid instance id (sorted first)
-    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t per = (q + warps - 1) / warps;
-    const uint64_t q0 = min(q, w * per), q1 = min(q, q0 + per);
-    BatchAnswerPolicy pol(sidx);
-    for (uint64_t a = q0; a < q1;) {
-        const uint32_t j = __ldg(sinst + a);
-        const uint64_t e = min(q1, (uint64_t)__ldg(bend + j));  // bend[j]: end of instance j's run
-        const uint64_t n = inst[j].S.g.n, b = inst[j].S.g.b;
-        const K *A = keys + inst[j].off;
-        if constexpr (GV > 0) {
-            if ((reinterpret_cast<uintptr_t>(A) & 15) == 0) {
-                btree_descend_warp<K, GV, 16 / sizeof(K), QK>(A, static_cast<const K *>(nullptr), 0, n, b, sq, a, e,
-                                                               ans, pol);
-                a = e;
-                continue;
-            }
-        }
-        btree_descend_warp<K, GS, 1, QK>(A, static_cast<const K *>(nullptr), 0, n, b, sq, a, e, ans, pol);
-        a = e;
     }
 }
 
@@ -901,39 +882,6 @@ int batch_query_workspace_bytes(const tl_batch_plan *plan, uint64_t q, uint64_t 
     return TL_SUCCESS;
 }
 
-// The cooperative batched query for b <= 32: G lanes per node chosen from b
-// and the key width, one launch over all sorted queries.
-template <typename K, int GV, int GS, int QK>
-static int launch_coop(const tl_batch_plan_impl &P, const K *keys, const K *sq, const uint32_t *sinst,
-                       const uint64_t *sidx, const unsigned long long *start, uint64_t q, uint64_t *ans,
-                       cudaStream_t st, int sms) {
-    auto kern = batch_query_coop_kernel<K, GV, GS, QK>;
-    int per_sm = 0;
-    TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchThreads, 0));
-    const uint64_t need = (q * GS / QK + kBatchThreads - 1) / kBatchThreads;
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)std::max(per_sm, 1) * sms));
-    kern<<<grid, kBatchThreads, 0, st>>>(keys, P.inst, sq, sinst, sidx, start, start + P.num, ans);
-    return TL_SUCCESS;
-}
-
-template <typename K>
-static int launch_batch_query_coop(const tl_batch_plan_impl &P, const K *keys, const K *sq, const uint32_t *sinst,
-                                   const uint64_t *sidx, const unsigned long long *start, uint64_t q, uint64_t *ans,
-                                   cudaStream_t st, int sms) {
-    const uint64_t b = P.b, nb = b * sizeof(K);
-    const uint64_t gv = nb % 16 == 0 ? nb / 16 : 0;  // 16-byte rows where the instance is aligned
-#define TL_BQ(GV, GS, QK) return launch_coop<K, GV, GS, QK>(P, keys, sq, sinst, sidx, start, q, ans, st, sms)
-    if (b == 1) TL_BQ(0, 1, 2);
-    if (b == 2) { if (gv == 1) TL_BQ(1, 2, 2); TL_BQ(0, 2, 2); }
-    if (b <= 4) { if (gv == 1) TL_BQ(1, 4, 4); if (gv == 2) TL_BQ(2, 4, 4); TL_BQ(0, 4, 4); }
-    if (b <= 8) { if (gv == 2) TL_BQ(2, 8, 4); if (gv == 4) TL_BQ(4, 8, 4); TL_BQ(0, 8, 4); }
-    if (b <= 16) { if (gv == 4) TL_BQ(4, 16, 4); if (gv == 8) TL_BQ(8, 16, 4); TL_BQ(0, 16, 4); }
-    if (gv == 8) TL_BQ(8, 32, 8);
-    if (gv == 16) TL_BQ(16, 32, 8);
-    TL_BQ(0, 32, 8);
-#undef TL_BQ
-}
-
 template <typename K>
 static int launch_batch_query(const tl_batch_plan_impl &P, const K *keys, const K *Q, const uint32_t *qinst,
                               uint64_t q, uint64_t *ans, char *ws, cudaStream_t st) {
@@ -953,16 +901,8 @@ static int launch_batch_query(const tl_batch_plan_impl &P, const K *keys, const 
     batch_scan_kernel<<<1, 1024, 0, st>>>(count, P.num, start);
     batch_bucket_kernel<K><<<g, 256, 0, st>>>(Q, qinst, q, P.num, start, sq, sinst, sidx);
     TL_CUDA_TRY(cudaGetLastError());
-    // after the bucket pass start[j] holds the end of bucket j.  Valid queries:
-    // start[num] (read on the device).
-    if (P.b <= 32) {
-        int rc = launch_batch_query_coop<K>(P, keys, sq, sinst, sidx, start, q, ans, st, sms);
-        if (rc) return rc;
-        TL_CUDA_TRY(cudaGetLastError());
-        return TL_SUCCESS;
-    }
-    // larger nodes: a thread per query scanning the node, the CTA's chunk
-    // pinning its instance's top levels in shared memory
+    // after the bucket pass start[j] holds the end of bucket j; the query kernel
+    // only needs the sorted arrays.  Valid queries: start[num] (read on device).
     const uint32_t pin_cap = (uint32_t)(48 * 1024 / sizeof(K));
     const size_t smem = (size_t)pin_cap * sizeof(K);
     auto kern = batch_query_kernel<K>;

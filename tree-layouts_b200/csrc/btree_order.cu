@@ -16,13 +16,15 @@
 // keys for the second pass.
 //
 // The tables depend on (n, b, tile_keys) only.  They are computed once on the
-// host (O(tiles): a few source runs per tile) and copied once to each device
+// host (O(tiles): a few source runs per tile; the per-tile passes and the two
+// tie orders on the host's threads) and copied once to each device
 // that uses them; both copies live until the process exits.  A geometry seen
 // for the first time while its stream is being captured gets no device copy
 // (the permutation then takes plan R or L).
 #include <algorithm>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "btree_order.h"
@@ -35,11 +37,34 @@ constexpr uint32_t kChainCap = 64;
 constexpr size_t kMaxOrderEntries = 64;
 constexpr int kMaxOrderDevices = 64;
 
+static void order_preds_range(const BtreeStream &S, std::vector<int64_t> &pred, uint64_t u0, uint64_t u1);
+
+// fn(u0, u1) over [0, N) in contiguous slices on the host's threads (one
+// slice per 4096 tiles at most, 16 threads at most).
+template <typename Fn>
+static void parallel_tiles(uint64_t N, Fn fn) {
+    const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t T = std::max<uint64_t>(1, std::min<uint64_t>({hw, 16, (N + 4095) / 4096}));
+    if (T == 1) {
+        fn(0, N);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (uint64_t t = 0; t < T; ++t) th.emplace_back(fn, N * t / T, N * (t + 1) / T);
+    for (auto &x : th) x.join();
+}
+
 // pred(u) for every tile: the source tile with the longest run into u.
 static void order_preds(const BtreeStream &S, std::vector<int64_t> &pred) {
-    const uint64_t N = S.ntiles, T = S.tile_keys, thr = T / 8;
+    const uint64_t N = S.ntiles;
     pred.assign(N, -1);
-    for (uint64_t u = 0; u < N; ++u) {
+    parallel_tiles(N, [&](uint64_t u0, uint64_t u1) { order_preds_range(S, pred, u0, u1); });
+}
+
+static void order_preds_range(const BtreeStream &S, std::vector<int64_t> &pred, uint64_t u0, uint64_t u1) {
+    const uint64_t T = S.tile_keys, thr = T / 8;
+    for (uint64_t u = u0; u < u1; ++u) {
         const uint64_t P0 = u << S.tile_shift, P1 = std::min(P0 + T, S.g.n);
         uint64_t best = 0;
         int64_t bz = -1;
@@ -89,14 +114,22 @@ static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, boo
         v.tab[u].x = (uint32_t)t;
     }
     S.tab = v.tab.data();
+    // scratch keys per tile (each tile's count depends on the ticket table only)
+    std::vector<uint32_t> cnt(N, 0);
+    parallel_tiles(N, [&](uint64_t u0, uint64_t u1) {
+        for (uint64_t u = u0; u < u1; ++u) {
+            uint64_t c = 0;
+            btree_fix_tile_host(S, u, [&](uint64_t, uint64_t len) {
+                c += len;
+                return true;
+            });
+            cnt[u] = (uint32_t)c;
+        }
+    });
     std::vector<uint8_t> full(N, 0);
     uint64_t keys = 0, slots = 0;
     for (uint64_t u = 0; u < N; ++u) {
-        uint64_t c = 0;
-        btree_fix_tile_host(S, u, [&](uint64_t, uint64_t len) {
-            c += len;
-            return true;
-        });
+        const uint64_t c = cnt[u];
         if (!c) continue;
         keys += c;
         v.tab[u].y = (uint32_t)slots++;
@@ -170,16 +203,14 @@ void btree_compute_order(const BtreeStream &S0, OrderVectors &v) {
             cur = std::min<uint32_t>(kChainCap, cur + 1);
         }
     }
-    // both tie orders (right to left, left to right); keep the one with fewer scratch keys
-    OrderVectors w;
-    uint64_t best = UINT64_MAX;
-    for (int asc = 0; asc < 2; ++asc) {
-        const uint64_t c = order_by_depth(S, m, asc != 0, w);
-        if (c < best) {
-            best = c;
-            std::swap(v, w);
-        }
-    }
+    // both tie orders (right to left, left to right), side by side; keep the
+    // one with fewer scratch keys (right to left on a tie)
+    OrderVectors w0, w1;
+    uint64_t c0 = 0, c1 = 0;
+    std::thread t1([&] { c1 = order_by_depth(S, m, true, w1); });
+    c0 = order_by_depth(S, m, false, w0);
+    t1.join();
+    std::swap(v, c1 < c0 ? w1 : w0);
 }
 
 namespace {

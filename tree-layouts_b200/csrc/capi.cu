@@ -5,6 +5,8 @@
 #include <cstring>
 
 #include "geometry.cuh"
+#include <utility>
+
 #include "internal.h"
 #include "learned.h"
 #include "stream.cuh"
@@ -184,6 +186,42 @@ int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t k
     return permute_scratch_keys(layout, n, b, key_bytes, keys);
 }
 
+// Measurement hook: query kernel variants (0: the default).
+void tl_debug_set_query_variant(int v) { set_query_variant(v); }
+
+// Test hook: host replay of the cycle-leader step list (and, for the hybrid
+// BST, the perfect part's two involutions as a host permutation).
+int tl_debug_emulate_algorithm(int layout, int algorithm, uint64_t n, uint64_t b, uint64_t *host_A,
+                               uint64_t *steps) {
+    if (!host_A && n) return TL_ERROR_INVALID_VALUE;
+    if (algorithm != TL_ALGO_CYCLES && algorithm != TL_ALGO_HYBRID) return TL_ERROR_INVALID_VALUE;
+    if (layout == TL_LAYOUT_BTREE && (b == 0 || b >= (1ull << 20))) return TL_ERROR_INVALID_VALUE;
+    if (n <= 1) return TL_SUCCESS;
+    uint64_t ni = 0;
+    int rc = emulate_cycles(layout, algorithm, n, b, host_A, &ni, steps);
+    if (rc || algorithm != TL_ALGO_HYBRID || ni <= 1) return rc;
+    // perfect BST of d levels on ranks 1..ni: rank x <-> its d-bit reversal,
+    // then x <-> x with its bits below the leading one reversed
+    uint32_t d = 0;
+    while ((1ull << d) <= ni) ++d;
+    auto rev = [](uint64_t x, uint32_t bits) {
+        uint64_t r = 0;
+        for (uint32_t t = 0; t < bits; ++t) r |= ((x >> t) & 1) << (bits - 1 - t);
+        return r;
+    };
+    for (uint64_t x = 1; x <= ni; ++x) {
+        const uint64_t y = rev(x, d);
+        if (x < y) std::swap(host_A[x - 1], host_A[y - 1]);
+    }
+    for (uint64_t x = 1; x <= ni; ++x) {
+        uint32_t lb = 0;
+        while ((x >> (lb + 1)) != 0) ++lb;  // position of the leading one
+        const uint64_t y = ((x >> lb) << lb) | rev(x & ((1ull << lb) - 1), lb);
+        if (x < y) std::swap(host_A[x - 1], host_A[y - 1]);
+    }
+    return TL_SUCCESS;
+}
+
 // Test hook: host replay of the permutation's tile schedule (see emulate_permute).
 int tl_debug_emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *host_A, uint64_t *violations) {
     if (n > 0 && !host_A) return TL_ERROR_INVALID_VALUE;
@@ -341,6 +379,11 @@ int tl_rank_model_train(const uint64_t *keys, uint64_t n, const tl_rank_train_co
                         tl_rank_leaf *leaves, void *stream) {
     return rank_model_train(keys, n, cfg, model, leaves, S(stream));
 }
+int tl_debug_rank_model_root(const tl_rank_model *model, const float *x, uint32_t count, float *out,
+                             uint32_t *pieces) {
+    return rank_model_root_eval(model, x, count, out, pieces);
+}
+
 int tl_rank_model_predict(const tl_rank_model *model, const tl_rank_leaf *leaves, const uint64_t *keys, uint64_t q,
                           uint64_t *rank, uint32_t *eps, void *stream) {
     return rank_model_predict(model, leaves, keys, q, rank, eps, S(stream));

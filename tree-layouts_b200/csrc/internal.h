@@ -103,6 +103,15 @@ int stream_blocks_per_sm(int layout, uint32_t key_bytes);
 int last_permute_launches();
 int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
 int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations);
+// query.cu: kernel selection for measurements (0: the default)
+void set_query_variant(int v);
+int query_variant();
+// cycles.cu: the cycle-leader family (and the hybrid BST's last level); for
+// the hybrid *perfect = keys of the front part the involutions finish
+int permute_cycles(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
+                   cudaStream_t st, uint64_t *perfect);
+int emulate_cycles(int layout, int algorithm, uint64_t n, uint64_t b, uint64_t *A, uint64_t *perfect,
+                   uint64_t *steps);
 int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_ws,
             uint64_t ws_bytes, cudaStream_t st, float *ms, float *phase_ms = nullptr, bool allow_ordered = true);
 

@@ -15,9 +15,11 @@
 // the query.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
+#include <memory>
+#include <vector>
 
-#include "descent.cuh"
 #include "geometry.cuh"
 #include "internal.h"
 #include "learned.h"
@@ -28,33 +30,132 @@ constexpr int H = TL_RMI_HIDDEN;
 constexpr int kParams = H + H + H * H + H + H + 1;  // w1 b1 w2 b2 w3 b3
 constexpr int kTrainThreads = 64;                  // samples per training block
 
-struct ModelParams {  // kernel-parameter copy of the root network (constant bank)
-    float w1[H], b1[H], w2[H][H], b2[H], w3[H], b3;
-    float2 w2p[H][H / 2];  // w2p[i][k] = (w2[2k][i], w2[2k+1][i]): the hidden layer two outputs at a time
-    float2 b2p[H / 2], w3p[H / 2];
+// The trained root network evaluated through its exact piecewise-linear form.
+// With one input and ReLU hidden layers the network is a continuous
+// piecewise-linear function of x: the first layer's units switch at most once
+// each (at x = -b1 / w1), and between two such points every second-layer
+// unit is affine in x and switches at most once more.  compile_root lists the
+// pieces (at most 33 * 33; start of each piece, slope, intercept) on the host
+// in double precision; inference finds x's piece by binary search in shared
+// memory and takes one FMA, where the layer-by-layer form takes about 1 100.
+// Every inference step - the leaf fit, the eps pass, prediction and the
+// queries - uses this one evaluator, so each leaf's eps bounds exactly what
+// the queries see.  Training itself runs the network layer by layer
+// (rmi_grad_kernel).
+constexpr uint32_t kMaxPieces = 1152;  // >= 33 * 33
+constexpr uint32_t kGridCells = 1024;  // uniform index over [0, 1]
+
+struct RootPieces {
+    uint32_t count;
+    float x0[kMaxPieces];  // piece k covers [x0[k], x0[k + 1]); x0[0] = 0
+    float s[kMaxPieces], t[kMaxPieces];
+    // first[c]: the piece holding c / kGridCells, so an x in cell c lies in a
+    // piece of first[c] .. first[c + 1]
+    uint16_t first[kGridCells + 1];
+};
+
+struct ModelParams {  // kernel-parameter copy of the inference model (constant bank)
+    RootPieces root;
     float x_lo, x_scale;
     uint32_t log_feature, num_leaves;
 };
 
+static void compile_root(const tl_rank_model &m, RootPieces &rp) {
+    std::vector<double> bp = {0.0, 1.0};
+    for (int i = 0; i < H; ++i)
+        if (m.w1[i] != 0.f) {
+            const double x = -(double)m.b1[i] / (double)m.w1[i];
+            if (x > 0.0 && x < 1.0) bp.push_back(x);
+        }
+    std::sort(bp.begin(), bp.end());
+    bp.erase(std::unique(bp.begin(), bp.end()), bp.end());
+    rp.count = 0;
+    std::vector<double> sub;
+    double A[H], C[H];
+    for (size_t iv = 0; iv + 1 < bp.size(); ++iv) {
+        const double a = bp[iv], c = bp[iv + 1], mid = 0.5 * (a + c);
+        for (int j = 0; j < H; ++j) {  // second-layer pre-activation = A_j x + C_j on (a, c)
+            A[j] = 0.0;
+            C[j] = (double)m.b2[j];
+            for (int i = 0; i < H; ++i)
+                if ((double)m.w1[i] * mid + (double)m.b1[i] > 0.0) {
+                    A[j] += (double)m.w2[j][i] * (double)m.w1[i];
+                    C[j] += (double)m.w2[j][i] * (double)m.b1[i];
+                }
+        }
+        sub.assign({a, c});
+        for (int j = 0; j < H; ++j)
+            if (A[j] != 0.0) {
+                const double x = -C[j] / A[j];
+                if (x > a && x < c) sub.push_back(x);
+            }
+        std::sort(sub.begin(), sub.end());
+        sub.erase(std::unique(sub.begin(), sub.end()), sub.end());
+        for (size_t k = 0; k + 1 < sub.size(); ++k) {
+            const double m2 = 0.5 * (sub[k] + sub[k + 1]);
+            double S = 0.0, T = (double)m.b3;
+            for (int j = 0; j < H; ++j)
+                if (A[j] * m2 + C[j] > 0.0) {
+                    S += (double)m.w3[j] * A[j];
+                    T += (double)m.w3[j] * C[j];
+                }
+            if (rp.count == kMaxPieces) return;  // cannot happen: at most 33 * 33 pieces
+            rp.x0[rp.count] = (float)sub[k];
+            rp.s[rp.count] = (float)S;
+            rp.t[rp.count] = (float)T;
+            ++rp.count;
+        }
+    }
+    rp.x0[0] = 0.f;
+    uint32_t k = 0;
+    for (uint32_t c = 0; c <= kGridCells; ++c) {
+        const float e = (float)c / (float)kGridCells;  // exact: kGridCells is a power of two
+        while (k + 1 < rp.count && rp.x0[k + 1] <= e) ++k;
+        rp.first[c] = (uint16_t)k;
+    }
+}
+
 static ModelParams to_params(const tl_rank_model &m) {
     ModelParams p;
-    memcpy(p.w1, m.w1, sizeof p.w1);
-    memcpy(p.b1, m.b1, sizeof p.b1);
-    memcpy(p.w2, m.w2, sizeof p.w2);
-    memcpy(p.b2, m.b2, sizeof p.b2);
-    memcpy(p.w3, m.w3, sizeof p.w3);
-    p.b3 = m.b3;
-    for (int i = 0; i < H; ++i)
-        for (int k = 0; k < H / 2; ++k) p.w2p[i][k] = make_float2(m.w2[2 * k][i], m.w2[2 * k + 1][i]);
-    for (int k = 0; k < H / 2; ++k) {
-        p.b2p[k] = make_float2(m.b2[2 * k], m.b2[2 * k + 1]);
-        p.w3p[k] = make_float2(m.w3[2 * k], m.w3[2 * k + 1]);
-    }
+    compile_root(m, p.root);
     p.x_lo = (float)m.x_lo;
     p.x_scale = (float)m.x_scale;
     p.log_feature = m.log_feature;
     p.num_leaves = m.num_leaves;
     return p;
+}
+
+// The pieces in shared memory (every thread of the block, before any use).
+struct PiecesSmem {
+    float x0[kMaxPieces], s[kMaxPieces], t[kMaxPieces];
+    uint16_t first[kGridCells + 1];
+};
+
+__device__ __forceinline__ void stage_pieces(const ModelParams &p, PiecesSmem &sp) {
+    for (uint32_t k = threadIdx.x; k < p.root.count; k += blockDim.x) {
+        sp.x0[k] = p.root.x0[k];
+        sp.s[k] = p.root.s[k];
+        sp.t[k] = p.root.t[k];
+    }
+    for (uint32_t c = threadIdx.x; c <= kGridCells; c += blockDim.x) sp.first[c] = p.root.first[c];
+    __syncthreads();
+}
+
+// The root's output at x in [0, 1]: the last piece starting at or below x,
+// found from x's grid cell (usually no further step; a binary search where
+// several pieces start inside one cell).
+TL_HD float pieces_eval(const float *x0, const float *s, const float *t, const uint16_t *first, float x) {
+    const uint32_t cf = (uint32_t)(x * (float)kGridCells);
+    const uint32_t c = cf < kGridCells ? cf : kGridCells - 1;
+    uint32_t lo = first[c], hi = first[c + 1];
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (x0[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return fmaf(s[lo], x, t[lo]);
 }
 
 // Normalised feature of a key, in [0, 1] over the trained key range:
@@ -71,27 +172,6 @@ __device__ __forceinline__ float feature(const ModelParams &p, uint64_t key) {
     return feature_x(p.log_feature, p.x_lo, p.x_scale, key);
 }
 
-// Root network output (predicted rank / n).  The hidden layer runs two output
-// units per packed FP32x2 FMA (sm_100's FFMA2), each lane a plain fmaf chain in
-// the same input order.
-__device__ __forceinline__ float root_forward(const ModelParams &p, float x) {
-    float2 acc[H / 2];
-#pragma unroll
-    for (int k = 0; k < H / 2; ++k) acc[k] = p.b2p[k];
-#pragma unroll
-    for (int i = 0; i < H; ++i) {
-        const float h = fmaxf(fmaf(p.w1[i], x, p.b1[i]), 0.f);
-        const float2 hh = make_float2(h, h);
-#pragma unroll
-        for (int k = 0; k < H / 2; ++k) acc[k] = __ffma2_rn(p.w2p[i][k], hh, acc[k]);
-    }
-    float2 o = make_float2(p.b3, 0.f);
-#pragma unroll
-    for (int k = 0; k < H / 2; ++k)
-        o = __ffma2_rn(p.w3p[k], make_float2(fmaxf(acc[k].x, 0.f), fmaxf(acc[k].y, 0.f)), o);
-    return o.x + o.y;
-}
-
 __device__ __forceinline__ uint32_t leaf_of(const ModelParams &p, float out) {
     float f = out * (float)p.num_leaves;
     if (!(f > 0.f)) return 0;  // also catches NaN
@@ -99,9 +179,29 @@ __device__ __forceinline__ uint32_t leaf_of(const ModelParams &p, float out) {
     return l < p.num_leaves ? l : p.num_leaves - 1;
 }
 
-// Leaf-only ablation: the root network replaced by the identity.
-__device__ __forceinline__ float root_eval(const ModelParams &p, float x, bool use_net) {
-    return use_net ? root_forward(p, x) : x;
+// The root's output (use_net) or, for the leaf-only ablation, x itself.
+__device__ __forceinline__ float root_eval(const ModelParams &p, const PiecesSmem &sp, float x, bool use_net) {
+    return use_net ? pieces_eval(sp.x0, sp.s, sp.t, sp.first, x) : x;
+}
+
+static_assert(sizeof(tl_rank_leaf) == 32 && offsetof(tl_rank_leaf, slope) == 16 &&
+                  offsetof(tl_rank_leaf, eps_lo) == 20 && offsetof(tl_rank_leaf, empty) == 28,
+              "load_leaf reads the segment entry as four 64-bit words");
+
+// A segment entry (32 bytes) in one load where the table is 32-byte aligned.
+__device__ __forceinline__ tl_rank_leaf load_leaf(const tl_rank_leaf *__restrict__ leaves, uint32_t l,
+                                                  bool aligned32) {
+    if (!aligned32) return leaves[l];
+    uint64_t w[4];
+    ldg32(reinterpret_cast<const uint64_t *>(leaves + l), w);
+    tl_rank_leaf lf;
+    lf.kmin = w[0];
+    lf.base = w[1];
+    lf.slope = __uint_as_float((uint32_t)w[2]);
+    lf.eps_lo = (uint32_t)(w[2] >> 32);
+    lf.eps_hi = (uint32_t)w[3];
+    lf.empty = (uint32_t)(w[3] >> 32);
+    return lf;
 }
 
 // Rank prediction of a segment, clamped to [0, n).
@@ -273,9 +373,11 @@ __global__ void rmi_adam_kernel(float *__restrict__ w, float *__restrict__ mom, 
 // atomics per change of leaf (the root is close to monotone, so runs are long).
 constexpr int kLeafChunk = 64;
 
-__global__ void leaf_extent_kernel(const ModelParams p, bool use_net, const uint64_t *__restrict__ keys,
+__global__ void leaf_extent_kernel(const __grid_constant__ ModelParams p, bool use_net, const uint64_t *__restrict__ keys,
                                    uint64_t n, unsigned long long *kmin, unsigned long long *kmax,
                                    unsigned long long *rmin, unsigned long long *rmax) {
+    __shared__ PiecesSmem sp;
+    if (use_net) stage_pieces(p, sp);
     const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c * kLeafChunk < n; c += nthr) {
         const uint64_t s0 = c * kLeafChunk, s1 = min(n, s0 + kLeafChunk);
@@ -286,7 +388,7 @@ __global__ void leaf_extent_kernel(const ModelParams p, bool use_net, const uint
             uint64_t k = 0;
             if (s < s1) {
                 k = keys[s];
-                l = leaf_of(p, root_eval(p, feature(p, k), use_net));
+                l = leaf_of(p, root_eval(p, sp, feature(p, k), use_net));
             }
             if (l != cur) {
                 if (cur != 0xFFFFFFFFu) {
@@ -333,8 +435,10 @@ __global__ void leaf_fit_kernel(uint32_t L, const unsigned long long *kmin, cons
 
 // The segment's error bounds: the largest over- and under-prediction over its
 // keys, computed with the inference arithmetic itself.
-__global__ void leaf_eps_kernel(const ModelParams p, bool use_net, const uint64_t *__restrict__ keys, uint64_t n,
+__global__ void leaf_eps_kernel(const __grid_constant__ ModelParams p, bool use_net, const uint64_t *__restrict__ keys, uint64_t n,
                                 tl_rank_leaf *leaves) {
+    __shared__ PiecesSmem sp;
+    if (use_net) stage_pieces(p, sp);
     const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c * kLeafChunk < n; c += nthr) {
         const uint64_t s0 = c * kLeafChunk, s1 = min(n, s0 + kLeafChunk);
@@ -343,7 +447,7 @@ __global__ void leaf_eps_kernel(const ModelParams p, bool use_net, const uint64_
             uint32_t l = 0xFFFFFFFFu, eo = 0, eu = 0;
             if (s < s1) {
                 const uint64_t k = keys[s];
-                l = leaf_of(p, root_eval(p, feature(p, k), use_net));
+                l = leaf_of(p, root_eval(p, sp, feature(p, k), use_net));
                 const uint64_t pr = leaf_predict(leaves[l], k, n);
                 const uint64_t d = pr > s ? pr - s : s - pr;
                 const uint32_t e = d > 0xFFFFFFFEull ? 0xFFFFFFFEu : (uint32_t)d;
@@ -365,13 +469,15 @@ __global__ void leaf_eps_kernel(const ModelParams p, bool use_net, const uint64_
     }
 }
 
-__global__ void rmi_predict_kernel(const ModelParams p, bool use_net, const tl_rank_leaf *__restrict__ leaves,
+__global__ void rmi_predict_kernel(const __grid_constant__ ModelParams p, bool use_net, const tl_rank_leaf *__restrict__ leaves,
                                    const uint64_t *__restrict__ keys, uint64_t nq, uint64_t n,
                                    uint64_t *__restrict__ rank, uint32_t *__restrict__ eps) {
+    __shared__ PiecesSmem sp;
+    if (use_net) stage_pieces(p, sp);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t k = keys[i];
-        const uint32_t l = leaf_of(p, root_eval(p, feature(p, k), use_net));
+        const uint32_t l = leaf_of(p, root_eval(p, sp, feature(p, k), use_net));
         const tl_rank_leaf lf = leaves[l];
         rank[i] = leaf_predict(lf, k, n);
         if (eps) eps[i] = lf.empty ? 0xFFFFFFFFu : max(lf.eps_lo, lf.eps_hi);
@@ -403,105 +509,243 @@ __device__ __forceinline__ void rank_gaps(const LearnedGeom &G, uint64_t s, uint
     }
 }
 
-// The learned start as a policy of the cooperative descent (descent.cuh).
-// prepare() runs the model for one query per lane and picks the start node;
-// a descent started below the root records whether it saw node keys on either
-// side of the query (flags kSeenLess / kSeenGreater) and, when it falls off the
-// tree without them, restarts from the root.
-constexpr uint32_t kSubtree = 1, kSeenLess = 2, kSeenGreater = 4;
-
-struct LearnedPolicy {
-    const LearnedGeom &G;
-    const ModelParams &p;
-    const tl_rank_leaf *__restrict__ leaves;
-    int use_net;
-    unsigned long long n_fallback = 0, depth_sum = 0;
-
-    __device__ LearnedPolicy(const LearnedGeom &g, const ModelParams &pp, const tl_rank_leaf *lv, int un)
-        : G(g), p(pp), leaves(lv), use_net(un) {}
-
-    template <typename K>
-    __device__ __forceinline__ QEntry prepare(const K *__restrict__ Q, uint64_t qi, bool valid) {
-        QEntry e;
-        e.valid = valid;
-        e.node = 0;
-        e.flags = 0;
-        e.key = 0;
-        if (!valid) return e;
-        const BtreeGeom &g = G.g;
-        const uint64_t n = g.n, B = g.b;
-        const K q = __ldcs(Q + qi);
-        e.key = (uint64_t)q;
-        // predicted rank window -> deepest subtree covering it
-        const uint32_t l = leaf_of(p, root_eval(p, feature(p, (uint64_t)q), use_net != 0));
-        const tl_rank_leaf lf = leaves[l];
-        if (!lf.empty && g.h > 0) {
-            const uint64_t pr = leaf_predict(lf, (uint64_t)q, n);
-            const uint64_t rlo = pr > lf.eps_lo ? pr - lf.eps_lo : 0;
-            const uint64_t rhi = pr + lf.eps_hi < n ? pr + lf.eps_hi : n - 1;
-            uint64_t glo, ghi, t0, t1;
-            rank_gaps(G, rlo, glo, t0);
-            rank_gaps(G, rhi, t1, ghi);
-            uint32_t k = g.h;  // depth of the subtree root (h = a last-level node)
-            while (glo != ghi) {
-                glo = G.fd.div(glo);
-                ghi = G.fd.div(ghi);
-                --k;
-            }
-            // a last-level node that does not exist: start one level up
-            if (k == g.h && !(glo < g.i || (glo == g.i && g.r > 0))) {
-                glo = G.fd.div(glo);
-                --k;
-            }
-            const uint64_t start = g.pw[k] - 1 + glo * B;
-            if (start < n) {
-                depth_sum += k;
-                e.node = start;
-                e.flags = kSubtree;
-                return e;
+// A node of B = NB / 8 keys (NB = b * 8 bytes): lt = keys < q, eq = a key == q,
+// valid = keys below n.  Full nodes by NB / VB independent VB-byte loads (VB =
+// 32 on a 32-byte aligned layout, else 16), the partial last leaf by guarded
+// scalar loads.
+template <int NB, int VB>
+__device__ __forceinline__ void node_scan(const uint64_t *__restrict__ A, uint64_t n, uint64_t i, uint64_t q,
+                                          uint32_t &lt, uint32_t &valid, bool &eq) {
+    constexpr int B = NB / 8, KPL = VB / 8, NL = NB / VB;
+    lt = 0;
+    eq = false;
+    if (i + B <= n) {
+        valid = B;
+        uint64_t v[NL][32 / 8];
+#pragma unroll
+        for (int j = 0; j < NL; ++j) {
+            if constexpr (VB == 32) {
+                ldg32(A + i + j * KPL, v[j]);
+            } else {
+                const uint4 x = __ldg(reinterpret_cast<const uint4 *>(A + i + j * KPL));
+                v[j][0] = ((uint64_t)x.y << 32) | x.x;
+                v[j][1] = ((uint64_t)x.w << 32) | x.z;
             }
         }
-        ++n_fallback;  // the plain search from the root
-        return e;
+#pragma unroll
+        for (int j = 0; j < NL; ++j)
+#pragma unroll
+            for (int e = 0; e < KPL; ++e) {
+                lt += v[j][e] < q;
+                eq |= v[j][e] == q;
+            }
+    } else {
+        valid = (uint32_t)(n - i);
+        for (uint32_t j = 0; j < valid; ++j) {
+            const uint64_t cur = __ldg(A + i + j);
+            lt += cur < q;
+            eq |= cur == q;
+        }
     }
-    __device__ __forceinline__ uint32_t seen(uint32_t flags, uint32_t lt, uint32_t cnt) const {
-        return flags | (lt > 0 ? kSeenLess : 0u) | (lt < cnt ? kSeenGreater : 0u);
-    }
-    // absent: the subtree held keys on both sides of the query; otherwise the
-    // window could not decide and the search restarts from the root
-    __device__ __forceinline__ bool fell_off(uint64_t &node, uint32_t &flags, bool leader) {
-        if (!(flags & kSubtree) || ((flags & kSeenLess) && (flags & kSeenGreater))) return true;
-        node = 0;
-        flags = 0;
-        if (leader) ++n_fallback;
-        return false;
-    }
-    __device__ __forceinline__ void answer(uint64_t *__restrict__ ans, uint64_t qi, uint64_t res) const {
-        __stcs(ans + qi, res);
-    }
-};
+}
 
-template <typename K, int G, int QK>
-__global__ void __launch_bounds__(256)
-learned_query_kernel(const K *__restrict__ A, const LearnedGeom LG, const __grid_constant__ ModelParams p,
-                     int use_net, const tl_rank_leaf *__restrict__ leaves, const K *__restrict__ Q, uint64_t nq,
-                     uint64_t *__restrict__ ans, unsigned long long *__restrict__ stats) {
+// A 16-key node (128 bytes, 32-byte aligned): four 32-byte loads, the quarter
+// holding q's rank from the three quarter maxima, then that quarter's keys
+// only (the keys are sorted: every key of an earlier quarter is below q).
+__device__ __forceinline__ void node_scan_quarters(const uint64_t *__restrict__ A, uint64_t n, uint64_t i, uint64_t q,
+                                                   uint32_t &lt, uint32_t &valid, bool &eq) {
+    if (i + 16 > n) {
+        node_scan<128, 32>(A, n, i, q, lt, valid, eq);
+        return;
+    }
+    valid = 16;
+    uint64_t v[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ldg32(A + i + j * 4, v[j]);
+    const uint32_t c = (v[0][3] < q) + (v[1][3] < q) + (v[2][3] < q);
+    uint64_t w[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) w[e] = c == 0 ? v[0][e] : c == 1 ? v[1][e] : c == 2 ? v[2][e] : v[3][e];
+    lt = 4 * c;
+    eq = false;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        lt += w[e] < q;
+        eq |= w[e] == q;
+    }
+}
+
+// The start of one query's descent: the deepest subtree whose in-order rank
+// range covers the model's window (flags kSubtree), or the root.
+constexpr uint32_t kSubtree = 1, kSeenLess = 2, kSeenGreater = 4;
+
+template <uint64_t B>
+__device__ __forceinline__ uint64_t learned_start(const LearnedGeom &G, const ModelParams &p, const PiecesSmem &sp,
+                                                  int use_net, const tl_rank_leaf *__restrict__ leaves, bool leaves32,
+                                                  uint64_t q, uint32_t &flags, uint32_t &depth) {
+    const BtreeGeom &g = G.g;
+    const uint64_t n = g.n;
+    flags = 0;
+    depth = 0;
+    const uint32_t l = leaf_of(p, root_eval(p, sp, feature(p, q), use_net != 0));
+    const tl_rank_leaf lf = load_leaf(leaves, l, leaves32);
+    if (lf.empty || g.h == 0) return 0;
+    const uint64_t pr = leaf_predict(lf, q, n);
+    const uint64_t rlo = pr > lf.eps_lo ? pr - lf.eps_lo : 0;
+    const uint64_t rhi = pr + lf.eps_hi < n ? pr + lf.eps_hi : n - 1;
+    uint64_t glo, ghi, t0, t1;
+    rank_gaps(G, rlo, glo, t0);
+    rank_gaps(G, rhi, t1, ghi);
+    uint32_t k = g.h;  // depth of the subtree root (h = a last-level node)
+    while (glo != ghi) {
+        glo = G.fd.div(glo);
+        ghi = G.fd.div(ghi);
+        --k;
+    }
+    // a last-level node that does not exist: start one level up
+    if (k == g.h && !(glo < g.i || (glo == g.i && g.r > 0))) {
+        glo = G.fd.div(glo);
+        --k;
+    }
+    const uint64_t i = g.pw[k] - 1 + glo * B;
+    if (i >= n) return 0;
+    flags = kSubtree;
+    depth = k;
+    return i;
+}
+
+constexpr uint64_t kIdle = ~0ull;
+
+// 1024-thread blocks: two per SM hold the pieces twice in shared memory (about
+// 30 KB), leaving the rest of the unified L1 to the descents' top levels (with
+// 256-thread blocks, eight copies took 143 KB of it and the descent slowed by
+// a quarter).
+#ifndef TL_LEARNED_THREADS
+#define TL_LEARNED_THREADS 1024
+#endif
+#ifndef TL_LEARNED_MIN_BLOCKS
+#define TL_LEARNED_MIN_BLOCKS 1
+#endif
+#ifndef TL_LEARNED_QUARTER
+#define TL_LEARNED_QUARTER 0
+#endif
+constexpr int kLearnedThreads = TL_LEARNED_THREADS;
+
+// One descent per lane, fed from a per-warp queue: a lane whose descent ends
+// takes the next prepared query at once, so start depths that differ, hits at
+// inner levels and the restarts from the root do not hold the warp's other
+// lanes (one query per lane at a time kept 12 of 32 lanes busy on average).
+// The queue holds 32 prepared starts, one per lane, computed together when it
+// runs dry (the rank model, the window and the start subtree, all lanes busy);
+// idle lanes take them in lane order by shuffle.  A descent started below the
+// root accepts a miss only when it saw node keys on both sides of the query
+// (kSeenLess, kSeenGreater); otherwise it restarts at the root.  Each warp
+// answers a contiguous range of the queries.
+template <int NB, int VB>
+__global__ void __launch_bounds__(kLearnedThreads, TL_LEARNED_MIN_BLOCKS)
+learned_query_kernel(const uint64_t *__restrict__ A, const LearnedGeom G, const __grid_constant__ ModelParams p,
+                     int use_net, const tl_rank_leaf *__restrict__ leaves, const uint64_t *__restrict__ Q,
+                     uint64_t nq, uint64_t *__restrict__ ans, unsigned long long *__restrict__ stats) {
+    constexpr uint64_t B = NB / 8;
+    __shared__ PiecesSmem sp;
+    if (use_net) stage_pieces(p, sp);
+    const bool leaves32 = (reinterpret_cast<uintptr_t>(leaves) & 31) == 0;
+    const uint64_t n = G.g.n;
+    const uint64_t cmax = (n + 1) / (B + 1);
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t per = (nq + warps - 1) / warps;
     const uint64_t q0 = min(nq, w * per), q1 = min(nq, q0 + per);
-    LearnedPolicy pol(LG, p, leaves, use_net);
-    btree_descend_warp<K, G, 16 / sizeof(K), QK>(A, static_cast<const K *>(nullptr), 0, LG.g.n, LG.g.b, Q, q0, q1, ans,
-                                                 pol);
+    unsigned long long n_fallback = 0, depth_sum = 0;
+    // this lane's descent
+    uint64_t node = kIdle, key = 0, qid = 0;
+    uint32_t fl = 0;
+    // this lane's prepared entry of the current batch
+    uint64_t e_node = 0, e_key = 0;
+    uint32_t e_fl = 0;
+    uint64_t next = q0, batch0 = q0;
+    uint32_t bn = 0, bpos = 0;
+    for (;;) {
+        unsigned need = __ballot_sync(0xFFFFFFFFu, node == kIdle);
+        while (need) {
+            if (bpos == bn) {
+                if (next >= q1) break;
+                batch0 = next;
+                bn = (uint32_t)(q1 - next < 32 ? q1 - next : 32);
+                bpos = 0;
+                next += bn;
+                if (lane < bn) {
+                    e_key = __ldcs(Q + batch0 + lane);
+                    uint32_t d;
+                    e_node = learned_start<B>(G, p, sp, use_net, leaves, leaves32, e_key, e_fl, d);
+                    if (e_fl) depth_sum += d; else ++n_fallback;
+                }
+            }
+            const uint32_t avail = bn - bpos;
+            unsigned take = need;
+            if ((uint32_t)__popc(need) > avail) {  // the lowest `avail` idle lanes
+                take = 0;
+                unsigned m = need;
+                for (uint32_t c = 0; c < avail; ++c) {
+                    const unsigned low = m & (0u - m);
+                    take |= low;
+                    m ^= low;
+                }
+            }
+            const bool mine = (take >> lane) & 1u;
+            const uint32_t src = bpos + __popc(take & below);
+            const uint64_t k2 = __shfl_sync(0xFFFFFFFFu, e_key, mine ? src : 0);
+            const uint64_t n2 = __shfl_sync(0xFFFFFFFFu, e_node, mine ? src : 0);
+            const uint32_t f2 = __shfl_sync(0xFFFFFFFFu, e_fl, mine ? src : 0);
+            if (mine) {
+                key = k2;
+                node = n2;
+                fl = f2;
+                qid = batch0 + src;
+            }
+            bpos += __popc(take);
+            need &= ~take;
+        }
+        if (!__any_sync(0xFFFFFFFFu, node != kIdle)) break;
+        if (node != kIdle) {
+            uint32_t lt, valid;
+            bool eq;
+            if (TL_LEARNED_QUARTER && NB == 128 && VB == 32)
+                node_scan_quarters(A, n, node, key, lt, valid, eq);
+            else
+                node_scan<NB, VB>(A, n, node, key, lt, valid, eq);
+            uint64_t res = kIdle;
+            if (eq) {
+                res = node + lt;
+            } else {
+                fl |= (lt > 0 ? kSeenLess : 0u) | (lt < valid ? kSeenGreater : 0u);
+                const uint64_t nx = node + 1 <= cmax ? (node + 1) * (B + 1) + (uint64_t)lt * B - 1 : n;
+                if (nx < n) {
+                    node = nx;
+                } else if (!(fl & kSubtree) || ((fl & kSeenLess) && (fl & kSeenGreater))) {
+                    res = n;  // absent (from the root; or the subtree straddles the query)
+                } else {      // the window could not decide: plain search from the root
+                    ++n_fallback;
+                    node = 0;
+                    fl = 0;
+                }
+            }
+            if (res != kIdle) {
+                __stcs(ans + qid, res);
+                node = kIdle;
+            }
+        }
+    }
     if (stats) {
-        unsigned long long f = pol.n_fallback, d = pol.depth_sum;
         for (int o = 16; o > 0; o >>= 1) {
-            f += __shfl_xor_sync(0xFFFFFFFFu, f, o);
-            d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
+            n_fallback += __shfl_xor_sync(0xFFFFFFFFu, n_fallback, o);
+            depth_sum += __shfl_xor_sync(0xFFFFFFFFu, depth_sum, o);
         }
         if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&stats[0], f);
-            atomicAdd(&stats[1], d);
+            atomicAdd(&stats[0], n_fallback);
+            atomicAdd(&stats[1], depth_sum);
         }
     }
 }
@@ -662,6 +906,15 @@ int rank_model_train(const uint64_t *keys, uint64_t n, const tl_rank_train_confi
     return TL_SUCCESS;
 }
 
+int rank_model_root_eval(const tl_rank_model *m, const float *x, uint32_t count, float *out, uint32_t *pieces) {
+    if (!m || (count && (!x || !out))) return TL_ERROR_INVALID_VALUE;
+    std::unique_ptr<RootPieces> rp(new RootPieces);
+    compile_root(*m, *rp);
+    for (uint32_t i = 0; i < count; ++i) out[i] = pieces_eval(rp->x0, rp->s, rp->t, rp->first, x[i]);
+    if (pieces) *pieces = rp->count;
+    return TL_SUCCESS;
+}
+
 int rank_model_predict(const tl_rank_model *m, const tl_rank_leaf *leaves, const uint64_t *keys, uint64_t q,
                        uint64_t *rank, uint32_t *eps, cudaStream_t st) {
     if (!m || !leaves || (q && (!keys || !rank))) return TL_ERROR_INVALID_VALUE;
@@ -677,8 +930,8 @@ int query_btree_learned(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank
                         unsigned long long *stats, cudaStream_t st, float *ms) {
     if (!m || !leaves || (q && (!Q || !ans)) || (n && !A)) return TL_ERROR_INVALID_VALUE;
     if (m->n != n) return TL_ERROR_INVALID_VALUE;
-    // cooperative node loads: b in {2, 4, 8, 16, 32, 64}, 16-byte aligned layout
-    if (b * 8 % 16 || b * 8 > 512 || ((b * 8 / 16) & (b * 8 / 16 - 1))) return TL_ERROR_UNSUPPORTED;
+    // vector node loads: b in {2, 4, 8, 16, 32} on a 16-byte aligned layout
+    if (b * 8 % 16 || b * 8 > 256 || ((b * 8 / 16) & (b * 8 / 16 - 1))) return TL_ERROR_UNSUPPORTED;
     if (reinterpret_cast<uintptr_t>(A) & 15) return TL_ERROR_INVALID_VALUE;
     if (q == 0) return TL_SUCCESS;
     LearnedGeom G;
@@ -692,20 +945,26 @@ int query_btree_learned(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank
     const ModelParams p = to_params(*m);
     const int use_net = m->train_root != 0;
     auto launch = [&](auto kern) -> int {
+        // the smallest shared-memory carve-out that holds the blocks' pieces:
+        // the rest stays L1
+        TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 15));
         int per_sm = 0;
-        TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
-        uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, (q + 63) / 64);
-        kern<<<(unsigned)std::max<uint64_t>(grid, 1), 256, 0, st>>>(A, G, p, use_net, leaves, Q, q, ans, stats);
+        TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLearnedThreads, 0));
+        uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms,
+                                           (q + kLearnedThreads - 1) / kLearnedThreads);
+        kern<<<(unsigned)std::max<uint64_t>(grid, 1), kLearnedThreads, 0, st>>>(A, G, p, use_net, leaves, Q, q, ans,
+                                                                               stats);
         return TL_SUCCESS;
     };
+    // 32-byte node loads on a 32-byte aligned layout (node bytes a multiple of 32), else 16-byte ones
+    const bool v32 = (reinterpret_cast<uintptr_t>(A) & 31) == 0 && (b * 8) % 32 == 0;
     int rc;
-    switch (b * 8 / 16) {
-        case 1: rc = launch(learned_query_kernel<uint64_t, 1, 2>); break;
-        case 2: rc = launch(learned_query_kernel<uint64_t, 2, 2>); break;
-        case 4: rc = launch(learned_query_kernel<uint64_t, 4, 4>); break;
-        case 8: rc = launch(learned_query_kernel<uint64_t, 8, 4>); break;
-        case 16: rc = launch(learned_query_kernel<uint64_t, 16, 8>); break;
-        case 32: rc = launch(learned_query_kernel<uint64_t, 32, 8>); break;
+    switch (b * 8) {
+        case 16: rc = launch(learned_query_kernel<16, 16>); break;
+        case 32: rc = v32 ? launch(learned_query_kernel<32, 32>) : launch(learned_query_kernel<32, 16>); break;
+        case 64: rc = v32 ? launch(learned_query_kernel<64, 32>) : launch(learned_query_kernel<64, 16>); break;
+        case 128: rc = v32 ? launch(learned_query_kernel<128, 32>) : launch(learned_query_kernel<128, 16>); break;
+        case 256: rc = v32 ? launch(learned_query_kernel<256, 32>) : launch(learned_query_kernel<256, 16>); break;
         default: return TL_ERROR_UNSUPPORTED;
     }
     if (rc) return rc;

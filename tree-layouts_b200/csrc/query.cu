@@ -11,7 +11,6 @@
 // the layout the descent visits the same nodes as the reference's searches.
 #include <algorithm>
 
-#include "descent.cuh"
 #include "internal.h"
 #include "tl_common.cuh"
 
@@ -173,23 +172,129 @@ btree_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_t P, 
     }
 }
 
-// The cooperative descent of descent.cuh: G lanes per node, KPL keys per lane,
-// QK descents in flight per group; contiguous query ranges per warp.  The top
-// levels (whole levels, the first P keys) are pinned in shared memory.
-template <typename K, int G, int KPL, int QK>
+// One thread per query, for nodes of b*w = 16*NV bytes (node starts are then
+// 16-byte aligned): the node is fetched with NV independent 16-byte loads.
+template <typename K, int NV>
 __global__ void __launch_bounds__(kQueryThreads)
-btree_query_coop_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_t P, const K *__restrict__ Q,
-                        uint64_t nq, uint64_t *__restrict__ ans) {
+btree_query_vec_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, const K *__restrict__ Q, uint64_t nq,
+                       uint64_t *__restrict__ ans) {
+    constexpr int KPV = 16 / sizeof(K);  // keys per 16-byte vector
+    constexpr int B = NV * KPV;          // == b
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t cmax = (n + 1) / (B + 1);
+    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
+        const K q = __ldcs(Q + qi);
+        uint64_t i = 0, res = n;
+        while (i < n) {
+            uint32_t lt = 0;
+            bool eq = false;
+            if (i + B <= n) {
+                const uint4 *node = reinterpret_cast<const uint4 *>(A + i);
+                uint4 v[NV];
+#pragma unroll
+                for (int j = 0; j < NV; ++j) v[j] = __ldg(node + j);
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+                    const K *kk = reinterpret_cast<const K *>(&v[j]);
+#pragma unroll
+                    for (int e = 0; e < KPV; ++e) lt += kk[e] < q;
+                }
+                if (lt < (uint32_t)B) {
+                    const K *all = reinterpret_cast<const K *>(v);
+                    K at = all[0];
+#pragma unroll
+                    for (int j = 1; j < B; ++j)
+                        if ((uint32_t)j == lt) at = all[j];
+                    eq = at == q;
+                }
+            } else {
+                const uint64_t valid = n - i;
+                for (uint64_t j = 0; j < valid; ++j) lt += __ldg(A + i + j) < q;
+                if (lt < valid) eq = __ldg(A + i + lt) == q;
+            }
+            if (eq) {
+                res = i + lt;
+                break;
+            }
+            if (i + 1 > cmax) break;
+            i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
+        }
+        __stcs(ans + qi, res);
+    }
+}
+
+// One thread per query for nodes of NB = b * w bytes, NB a multiple of 32 on a
+// 32-byte aligned layout: a node is NB / 32 independent 32-byte loads (one L1
+// wavefront each when the warp's nodes are distinct lines, half the 16-byte
+// loads' count).  The first P keys (whole top levels) may be pinned in shared
+// memory.  The partial last leaf is read with guarded scalar loads.
+template <typename K, int NB, bool kPin>
+__global__ void __launch_bounds__(kQueryThreads)
+btree_query_v32_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, const K *__restrict__ Q, uint64_t nq,
+                       uint64_t *__restrict__ ans) {
+    constexpr int KPL = 32 / sizeof(K);  // keys per 32-byte load
+    constexpr int NL = NB / 32;          // loads per node
+    constexpr int B = NB / sizeof(K);    // == b
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sm = reinterpret_cast<K *>(smem_raw);
-    pin_prefix(A, P, sm);
-    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t per = (nq + warps - 1) / warps;
-    const uint64_t q0 = min(nq, w * per), q1 = min(nq, q0 + per);
-    PlainPolicy pol;
-    btree_descend_warp<K, G, KPL, QK>(A, sm, P, n, b, Q, q0, q1, ans, pol);
+    if constexpr (kPin) pin_prefix(A, P, sm);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t cmax = (n + 1) / (B + 1);
+    for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += stride) {
+        const K q = __ldcs(Q + qi);
+        uint64_t i = 0, res = n;
+        while (i < n) {
+            uint32_t lt = 0;
+            bool eq = false;
+            if (i + B <= n) {
+                K v[NL][KPL];
+                if (kPin && i < P) {
+#pragma unroll
+                    for (int j = 0; j < NL; ++j) {
+                        const uint4 *s4 = reinterpret_cast<const uint4 *>(sm + i + j * KPL);
+                        const uint4 a = s4[0], c = s4[1];
+                        const K *ka = reinterpret_cast<const K *>(&a);
+                        const K *kc = reinterpret_cast<const K *>(&c);
+#pragma unroll
+                        for (int e = 0; e < KPL / 2; ++e) {
+                            v[j][e] = ka[e];
+                            v[j][KPL / 2 + e] = kc[e];
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NL; ++j) ldg32(A + i + j * KPL, v[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < NL; ++j)
+#pragma unroll
+                    for (int e = 0; e < KPL; ++e) lt += v[j][e] < q;
+#pragma unroll
+                for (int j = 0; j < NL; ++j)
+#pragma unroll
+                    for (int e = 0; e < KPL; ++e) eq |= v[j][e] == q;
+            } else {
+                const uint64_t valid = n - i;
+                for (uint64_t j = 0; j < valid; ++j) {
+                    const K cur = __ldg(A + i + j);
+                    lt += cur < q;
+                    eq |= cur == q;
+                }
+            }
+            if (eq) {
+                res = i + lt;
+                break;
+            }
+            if (i + 1 > cmax) break;
+            i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
+        }
+        __stcs(ans + qi, res);
+    }
 }
+
+static int g_query_variant = 0;
+void set_query_variant(int v) { g_query_variant = v; }
+int query_variant() { return g_query_variant; }
 
 // ---------------------------------------------------------------- mvEB
 // searchvEB (gpu/src/query-mveb.cuh:43-66): BFS index i and the table recurrence
@@ -198,8 +303,6 @@ btree_query_coop_kernel(const K *__restrict__ A, uint64_t n, uint64_t b, uint64_
 // read-only cache.  A descent past the deepest level ends as "absent" (the
 // reference reads past its table there; it only ever issues hits).
 constexpr int kVebThreads = 128;
-constexpr int kVebQueries = 4;                  // descents in flight per thread
-constexpr size_t kVebSmem = 110 * 1024;         // shared memory per block: pos[] + pinned prefix
 constexpr size_t kVebMinPin = 8 * 1024;
 
 // QK descents per thread in lock-step: every step takes all of a thread's
@@ -375,76 +478,107 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
         }
         P = std::min<uint64_t>(top, a.n);
         size_t smem = P * sizeof(K);
-        // 16-byte rows (b * w = 16 G on an aligned layout), else one key per
-        // lane for b <= 32, else the scalar group kernel below
+        // a thread per query with 32-byte node loads (b * w a multiple of 32 on
+        // a 32-byte aligned layout), else 16-byte ones (b * w a multiple of
+        // 16), else a group of lanes per query with one key per lane
         const uint64_t node_bytes = a.b * sizeof(K);
-        const uint64_t gv = node_bytes % 16 == 0 ? node_bytes / 16 : 0;
-        const bool aligned = (reinterpret_cast<uintptr_t>(A) & 15) == 0;
-        constexpr int KV = 16 / sizeof(K);
+        const uintptr_t base = reinterpret_cast<uintptr_t>(A);
         int rc = TL_SUCCESS;
         bool done = false;
-#define TL_BC(GG, KK, QK)                                                                  \
-    {                                                                                      \
-        auto kern = btree_query_coop_kernel<K, GG, KK, QK>;                                \
-        rc = persistent_grid(kern, smem, a.q * GG / QK, &grid);                            \
-        if (rc) return rc;                                                                 \
-        kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, a.b, P, Q, a.q, a.answers);        \
-        done = true;                                                                       \
-    }
-        if (aligned && (gv == 1 || gv == 2 || gv == 4 || gv == 8 || gv == 16 || gv == 32)) {
-            switch (gv) {
-                case 1: TL_BC(1, KV, 2) break;
-                case 2: TL_BC(2, KV, 2) break;
-                case 4: TL_BC(4, KV, 4) break;
-                case 8: TL_BC(8, KV, 4) break;
-                case 16: TL_BC(16, KV, 8) break;
-                case 32: TL_BC(32, KV, 8) break;
+        auto v32 = [&](auto kern, bool pin) -> int {
+            rc = persistent_grid(kern, pin ? smem : 0, a.q, &grid);
+            if (rc) return rc;
+            kern<<<grid, kQueryThreads, pin ? smem : 0, st>>>(A, a.n, pin ? P : 0, Q, a.q, a.answers);
+            done = true;
+            return TL_SUCCESS;
+        };
+        auto v16 = [&](auto kern) -> int {
+            rc = persistent_grid(kern, 0, a.q, &grid);
+            if (rc) return rc;
+            kern<<<grid, kQueryThreads, 0, st>>>(A, a.n, a.b, Q, a.q, a.answers);
+            done = true;
+            return TL_SUCCESS;
+        };
+        const bool pin = g_query_variant == 5;
+        if ((base & 31) == 0 && node_bytes % 32 == 0 && g_query_variant != 2) {
+            switch (node_bytes) {
+                case 32: rc = pin ? v32(btree_query_v32_kernel<K, 32, true>, true) : v32(btree_query_v32_kernel<K, 32, false>, false); break;
+                case 64: rc = pin ? v32(btree_query_v32_kernel<K, 64, true>, true) : v32(btree_query_v32_kernel<K, 64, false>, false); break;
+                case 128: rc = pin ? v32(btree_query_v32_kernel<K, 128, true>, true) : v32(btree_query_v32_kernel<K, 128, false>, false); break;
+                case 256: rc = pin ? v32(btree_query_v32_kernel<K, 256, true>, true) : v32(btree_query_v32_kernel<K, 256, false>, false); break;
+                default: break;
             }
-        } else if (a.b <= 32) {
-            if (a.b == 1) TL_BC(1, 1, 2)
-            else if (a.b == 2) TL_BC(2, 1, 2)
-            else if (a.b <= 4) TL_BC(4, 1, 4)
-            else if (a.b <= 8) TL_BC(8, 1, 4)
-            else if (a.b <= 16) TL_BC(16, 1, 4)
-            else TL_BC(32, 1, 8)
         }
-#undef TL_BC
+        if (!done && (base & 15) == 0 && node_bytes % 16 == 0) {
+            switch (node_bytes / 16) {
+                case 1: rc = v16(btree_query_vec_kernel<K, 1>); break;
+                case 2: rc = v16(btree_query_vec_kernel<K, 2>); break;
+                case 4: rc = v16(btree_query_vec_kernel<K, 4>); break;
+                case 8: rc = v16(btree_query_vec_kernel<K, 8>); break;
+                case 16: rc = v16(btree_query_vec_kernel<K, 16>); break;
+                default: break;
+            }
+        }
+        if (rc) return rc;
         if (done) {
             TL_CUDA_TRY(cudaGetLastError());
             return TL_SUCCESS;
         }
-        {  // b > 32 without 16-byte rows: 32 lanes, several slots per lane
-            auto kern = btree_query_kernel<K, 32>;
-            rc = persistent_grid(kern, smem, a.q * 32, &grid);
-            if (rc) return rc;
-            kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, a.b, P, Q, a.q, a.answers);
+        int G = 1;
+        while (G < 32 && (uint64_t)G < a.b) G <<= 1;
+#define TL_BT(GG)                                                                          \
+    case GG: {                                                                             \
+        auto kern = btree_query_kernel<K, GG>;                                             \
+        rc = persistent_grid(kern, smem, a.q * GG, &grid);                                 \
+        if (rc) return rc;                                                                 \
+        kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, a.b, P, Q, a.q, a.answers);        \
+        break;                                                                             \
+    }
+        switch (G) {
+            TL_BT(1)
+            TL_BT(2)
+            TL_BT(4)
+            TL_BT(8)
+            TL_BT(16)
+            TL_BT(32)
         }
+#undef TL_BT
     } else {
         const uint32_t dmax = bit_length(a.n);
         if (dmax > 63) return TL_ERROR_UNSUPPORTED;
         const bool np = a.layout == Q_VEB_NP;
         const bool narrow = a.n < (1ull << 32);
-        // kVebQueries columns of pos[] per thread; the layout's first positions
-        // pinned in what is left of kVebSmem (two blocks per SM)
-        const size_t pos_bytes = (size_t)dmax * kVebQueries * kVebThreads * (narrow ? 4 : 8);
-        const size_t pin_budget = pos_bytes + kVebMinPin <= kVebSmem ? kVebSmem - pos_bytes : kVebMinPin;
+        // QK columns of pos[] per thread; the layout's first positions pinned
+        // in what is left of the block's shared-memory budget
+        // one descent per thread: measured faster on B200 than two or four in
+        // lock-step (2^27 queries over 2^30 - 1 u32 keys: 40.5 ms against 55.5
+        // and 55.6; over 3e8 keys 36.6 against 49.0 and 49.3)
+        const int qk = g_query_variant == 3 ? 2 : g_query_variant == 4 ? 4 : 1;
+        const size_t budget = qk == 1 ? 48 * 1024 : qk == 2 ? 72 * 1024 : 110 * 1024;
+        const size_t pos_bytes = (size_t)dmax * qk * kVebThreads * (narrow ? 4 : 8);
+        const size_t pin_budget = pos_bytes + kVebMinPin <= budget ? budget - pos_bytes : kVebMinPin;
         P = std::min<uint64_t>(a.n, pin_budget / sizeof(K));
         const size_t smem = (pos_bytes + 15) / 16 * 16 + P * sizeof(K);
         if (smem > 227 * 1024) return TL_ERROR_UNSUPPORTED;  // pos[] of a tree deeper than about 50 levels
-        auto launch = [&](auto kern) -> int {
+        auto launch = [&](auto kern, int qpt) -> int {
             TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int per_sm = 0;
             TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kVebThreads, smem));
             uint64_t g = (uint64_t)std::max(per_sm, 1) * query_sm_count();
-            uint64_t need = (a.q + kVebQueries * kVebThreads - 1) / (kVebQueries * kVebThreads);
+            uint64_t need = (a.q + (uint64_t)qpt * kVebThreads - 1) / ((uint64_t)qpt * kVebThreads);
             unsigned gr = (unsigned)std::max<uint64_t>(1, std::min(g, need));
             kern<<<gr, kVebThreads, smem, st>>>(A, a.n, P, dmax, a.tables, np ? a.idx : nullptr,
                                                 np ? a.table_idx : nullptr, np ? a.num_tables : 1u, Q, a.q,
                                                 a.answers);
             return TL_SUCCESS;
         };
-        int rc = narrow ? launch(veb_query_kernel<K, uint32_t, kVebQueries>)
-                        : launch(veb_query_kernel<K, uint64_t, kVebQueries>);
+        int rc;
+        if (qk == 1)
+            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 1>, 1) : launch(veb_query_kernel<K, uint64_t, 1>, 1);
+        else if (qk == 2)
+            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 2>, 2) : launch(veb_query_kernel<K, uint64_t, 2>, 2);
+        else
+            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 4>, 4) : launch(veb_query_kernel<K, uint64_t, 4>, 4);
         if (rc) return rc;
     }
     TL_CUDA_TRY(cudaGetLastError());

@@ -72,4 +72,31 @@ TL_HD uint32_t bit_length(uint64_t x) {
 
 TL_HD uint64_t low_mask(uint32_t bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1); }
 
+// 32 bytes of keys in one load through the read-only path (sm_100's 256-bit
+// global loads); p 32-byte aligned.
+template <typename K>
+__device__ __forceinline__ void ldg32(const K *p, K (&out)[32 / sizeof(K)]) {
+    if constexpr (sizeof(K) == 8) {
+        unsigned long long a, b, c, d;
+        asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+        out[0] = a;
+        out[1] = b;
+        out[2] = c;
+        out[3] = d;
+    } else {
+        unsigned x0, x1, x2, x3, x4, x5, x6, x7;
+        asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=r"(x0), "=r"(x1), "=r"(x2), "=r"(x3), "=r"(x4), "=r"(x5), "=r"(x6), "=r"(x7)
+            : "l"(p));
+        out[0] = x0;
+        out[1] = x1;
+        out[2] = x2;
+        out[3] = x3;
+        out[4] = x4;
+        out[5] = x5;
+        out[6] = x6;
+        out[7] = x7;
+    }
+}
+
 }  // namespace tl

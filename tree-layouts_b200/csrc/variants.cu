@@ -7,7 +7,8 @@
 // restating the published method of Berney and Sitchinava): every step is a
 // self-inverse permutation applied by independent swaps, so each is one
 // grid-wide launch with no scratch and no waits.  (mvEB: see mveb_involutions
-// below.)  Not built: the cycle-leader family and the hybrid BST.
+// below.)  The cycle-leader family and the hybrid BST's last level are in
+// cycles.cu; the hybrid's perfect part is bst_perfect_involutions below.
 // BST:
 //  - perfect tree, n = 2^d - 1, ranks r = i + 1 in [1, 2^d - 1]: swap r with its
 //    d-bit reversal, then with r's bits below its leading one reversed;
@@ -182,6 +183,19 @@ static int bst_involutions(K *A, uint64_t n, cudaStream_t st) {
     return TL_SUCCESS;
 }
 
+// The perfect BST of ni = 2^d - 1 front keys by its two involutions (the
+// hybrid BST's second part, gpu/src/bst-hybrid.cuh:93-112).
+template <typename K>
+static int bst_perfect_involutions(K *A, uint64_t ni, cudaStream_t st) {
+    if (ni <= 1) return TL_SUCCESS;
+    uint32_t d = 0;
+    while ((1ull << d) <= ni) ++d;
+    bst_bitrev_kernel<K><<<grid_for(ni), kVariantThreads, 0, st>>>(A, ni, d);
+    bst_lowrev_kernel<K><<<grid_for(ni), kVariantThreads, 0, st>>>(A, ni);
+    TL_CUDA_TRY(cudaGetLastError());
+    return TL_SUCCESS;
+}
+
 // k-way shuffle (the N / k keys of each residue class interleaved back) and
 // its inverse, N a multiple of k: two modular involutions on [1, N - 1).  On
 // `parts` arrays of N keys at A + p * pstride + o (o = -1: an array that
@@ -339,9 +353,12 @@ static int mveb_involutions_run(K *A, uint64_t n, cudaStream_t st) {
 int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
                       cudaStream_t st, float *ms) {
     if (algorithm == TL_ALGO_STREAM) return permute(layout, dev_A, n, b, key_bytes, nullptr, 0, st, ms);
-    if (algorithm != TL_ALGO_INVOLUTIONS) return TL_ERROR_INVALID_VALUE;
+    if (algorithm < TL_ALGO_INVOLUTIONS || algorithm > TL_ALGO_HYBRID) return TL_ERROR_INVALID_VALUE;
+    if (layout < TL_LAYOUT_BST || layout > TL_LAYOUT_VEB) return TL_ERROR_INVALID_VALUE;
     if (layout == TL_LAYOUT_VEB) return TL_ERROR_UNSUPPORTED;  // the reference has it on the CPU only
+    if (algorithm == TL_ALGO_HYBRID && layout != TL_LAYOUT_BST) return TL_ERROR_UNSUPPORTED;
     if (layout == TL_LAYOUT_BTREE && (b == 0 || b >= (1ull << 31))) return TL_ERROR_INVALID_VALUE;
+    if (algorithm == TL_ALGO_CYCLES && layout == TL_LAYOUT_BTREE && b >= (1ull << 20)) return TL_ERROR_UNSUPPORTED;
     if (key_bytes != 4 && key_bytes != 8) return TL_ERROR_INVALID_VALUE;
     if (n > 0 && !dev_A) return TL_ERROR_INVALID_VALUE;
     if (reinterpret_cast<uintptr_t>(dev_A) % key_bytes) return TL_ERROR_INVALID_VALUE;
@@ -353,7 +370,15 @@ int permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uint64
     EventTimer timer(ms != nullptr, st);
     timer.start();
     int rc = TL_SUCCESS;
-    if (layout == TL_LAYOUT_BST) {
+    if (algorithm == TL_ALGO_CYCLES) {
+        rc = permute_cycles(layout, algorithm, dev_A, n, b, key_bytes, st, nullptr);
+    } else if (algorithm == TL_ALGO_HYBRID) {
+        uint64_t ni = 0;
+        rc = permute_cycles(layout, algorithm, dev_A, n, b, key_bytes, st, &ni);
+        if (!rc)
+            rc = key_bytes == 8 ? bst_perfect_involutions(static_cast<uint64_t *>(dev_A), ni, st)
+                                : bst_perfect_involutions(static_cast<uint32_t *>(dev_A), ni, st);
+    } else if (layout == TL_LAYOUT_BST) {
         rc = key_bytes == 8 ? bst_involutions(static_cast<uint64_t *>(dev_A), n, st)
                             : bst_involutions(static_cast<uint32_t *>(dev_A), n, st);
     } else if (layout == TL_LAYOUT_BTREE) {

@@ -126,6 +126,18 @@ def emulate_permute(layout: str, keys: np.ndarray, b: int = 16):
     return A, viol.value
 
 
+def emulate_algorithm(layout: str, algorithm: str, keys: np.ndarray, b: int = 16):
+    """Host replay of tl_permute_algorithm's steps for "cycles" / "hybrid";
+    returns (layout array, number of steps)."""
+    L = lib()
+    L.tl_debug_emulate_algorithm.argtypes = [C.c_int, C.c_int, _u64, _u64, _v, C.POINTER(_u64)]
+    A = np.ascontiguousarray(keys, dtype=np.uint64).copy()
+    steps = _u64()
+    _check(L.tl_debug_emulate_algorithm(LAYOUTS[layout], ALGORITHMS[algorithm], len(A), b, A.ctypes.data,
+                                        C.byref(steps)), "tl_debug_emulate_algorithm")
+    return A, steps.value
+
+
 def emulate_unpermute(layout: str, A: np.ndarray, b: int = 16) -> np.ndarray:
     """Host replay of the reverse permutation's gather; returns the sorted array."""
     out = np.ascontiguousarray(A, dtype=np.uint64).copy()
@@ -187,12 +199,14 @@ def permute(layout: str, keys, b: int = 16, stream=None, workspace=None, timed: 
     return ms.value if timed else None
 
 
-ALGORITHMS = {"stream": 0, "involutions": 1}
+ALGORITHMS = {"stream": 0, "involutions": 1, "cycles": 2, "hybrid": 3}
 
 
 def permute_algorithm(layout: str, algorithm: str, keys, b: int = 16, stream=None, timed: bool = False):
     """tl_permute_algorithm: the layout by one of the reference's algorithm
-    families ("involutions": BST, B-tree, mvEB) or by this library's own ("stream")."""
+    families ("involutions": BST, B-tree, mvEB; "cycles": the cycle-leader
+    family, BST, B-tree, mvEB; "hybrid": the BST by cycles and involutions) or
+    by this library's own ("stream")."""
     ms = C.c_float(0.0)
     rc = lib().tl_permute_algorithm(LAYOUTS[layout], ALGORITHMS[algorithm], keys.data_ptr(), keys.numel(), b,
                                     _key_bytes(keys), _stream_ptr(stream), C.byref(ms) if timed else None)
