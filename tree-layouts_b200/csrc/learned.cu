@@ -205,11 +205,13 @@ __device__ __forceinline__ tl_rank_leaf load_leaf(const tl_rank_leaf *__restrict
 }
 
 // Rank prediction of a segment, clamped to [0, n).
+// The segment's base rank stays an integer and only the offset within the
+// segment is FP32 (the base itself in FP32 would round to 64 ranks near 2^30,
+// and that rounding would widen every window).
 __device__ __forceinline__ uint64_t leaf_predict(const tl_rank_leaf &lf, uint64_t key, uint64_t n) {
-    float off = key > lf.kmin ? (float)(key - lf.kmin) : 0.f;
-    float r = (float)lf.base + lf.slope * off;
-    if (!(r > 0.f)) return 0;
-    uint64_t ri = (uint64_t)(r + 0.5f);
+    const float off = key > lf.kmin ? (float)(key - lf.kmin) : 0.f;
+    const float d = lf.slope * off;  // >= 0: slopes are non-negative
+    const uint64_t ri = lf.base + (d > 0.f ? (uint64_t)(d + 0.5f) : 0ull);
     return ri < n ? ri : n - 1;
 }
 
@@ -629,6 +631,7 @@ constexpr uint64_t kIdle = ~0ull;
 #ifndef TL_LEARNED_QUARTER
 #define TL_LEARNED_QUARTER 0
 #endif
+
 constexpr int kLearnedThreads = TL_LEARNED_THREADS;
 
 // One descent per lane, fed from a per-warp queue: a lane whose descent ends
@@ -647,6 +650,8 @@ learned_query_kernel(const uint64_t *__restrict__ A, const LearnedGeom G, const 
                      int use_net, const tl_rank_leaf *__restrict__ leaves, const uint64_t *__restrict__ Q,
                      uint64_t nq, uint64_t *__restrict__ ans, unsigned long long *__restrict__ stats) {
     constexpr uint64_t B = NB / 8;
+    // a descent's node index with its flags in the top bits (n < 2^61)
+    constexpr uint64_t kFlagShift = 61, kNodeMask = (1ull << kFlagShift) - 1;
     __shared__ PiecesSmem sp;
     if (use_net) stage_pieces(p, sp);
     const bool leaves32 = (reinterpret_cast<uintptr_t>(leaves) & 31) == 0;
@@ -656,31 +661,29 @@ learned_query_kernel(const uint64_t *__restrict__ A, const LearnedGeom G, const 
     const unsigned below = (1u << lane) - 1u;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t per = (nq + warps - 1) / warps;
-    const uint64_t q0 = min(nq, w * per), q1 = min(nq, q0 + per);
-    unsigned long long n_fallback = 0, depth_sum = 0;
-    // this lane's descent
-    uint64_t node = kIdle, key = 0, qid = 0;
-    uint32_t fl = 0;
-    // this lane's prepared entry of the current batch
-    uint64_t e_node = 0, e_key = 0;
-    uint32_t e_fl = 0;
-    uint64_t next = q0, batch0 = q0;
-    uint32_t bn = 0, bpos = 0;
+    const uint64_t per = (nq + warps - 1) / warps;  // below 2^32 (the host checks q)
+    const uint64_t q0 = min(nq, w * per);
+    const uint32_t cnt = (uint32_t)(min(nq, q0 + per) - q0);  // the warp's queries: q0 .. q0 + cnt
+    uint32_t n_fallback = 0, depth_sum = 0;
+    uint64_t cur = kIdle, key = 0;  // this lane's descent: node | flags << kFlagShift
+    uint32_t qoff = 0;
+    uint64_t e_cur = 0, e_key = 0;  // this lane's prepared entry of the current batch
+    uint32_t next = 0, batch0 = 0, bn = 0, bpos = 0;
     for (;;) {
-        unsigned need = __ballot_sync(0xFFFFFFFFu, node == kIdle);
+        unsigned need = __ballot_sync(0xFFFFFFFFu, cur == kIdle);
         while (need) {
             if (bpos == bn) {
-                if (next >= q1) break;
+                if (next >= cnt) break;
                 batch0 = next;
-                bn = (uint32_t)(q1 - next < 32 ? q1 - next : 32);
+                bn = cnt - next < 32 ? cnt - next : 32;
                 bpos = 0;
                 next += bn;
                 if (lane < bn) {
-                    e_key = __ldcs(Q + batch0 + lane);
-                    uint32_t d;
-                    e_node = learned_start<B>(G, p, sp, use_net, leaves, leaves32, e_key, e_fl, d);
-                    if (e_fl) depth_sum += d; else ++n_fallback;
+                    e_key = __ldcs(Q + q0 + batch0 + lane);
+                    uint32_t f, d;
+                    const uint64_t nd = learned_start<B>(G, p, sp, use_net, leaves, leaves32, e_key, f, d);
+                    e_cur = nd | ((uint64_t)f << kFlagShift);
+                    if (f) depth_sum += d; else ++n_fallback;
                 }
             }
             const uint32_t avail = bn - bpos;
@@ -697,25 +700,22 @@ learned_query_kernel(const uint64_t *__restrict__ A, const LearnedGeom G, const 
             const bool mine = (take >> lane) & 1u;
             const uint32_t src = bpos + __popc(take & below);
             const uint64_t k2 = __shfl_sync(0xFFFFFFFFu, e_key, mine ? src : 0);
-            const uint64_t n2 = __shfl_sync(0xFFFFFFFFu, e_node, mine ? src : 0);
-            const uint32_t f2 = __shfl_sync(0xFFFFFFFFu, e_fl, mine ? src : 0);
+            const uint64_t c2 = __shfl_sync(0xFFFFFFFFu, e_cur, mine ? src : 0);
             if (mine) {
                 key = k2;
-                node = n2;
-                fl = f2;
-                qid = batch0 + src;
+                cur = c2;
+                qoff = batch0 + src;
             }
             bpos += __popc(take);
             need &= ~take;
         }
-        if (!__any_sync(0xFFFFFFFFu, node != kIdle)) break;
-        if (node != kIdle) {
+        if (!__any_sync(0xFFFFFFFFu, cur != kIdle)) break;
+        if (cur != kIdle) {
+            const uint64_t node = cur & kNodeMask;
+            uint32_t fl = (uint32_t)(cur >> kFlagShift);
             uint32_t lt, valid;
             bool eq;
-            if (TL_LEARNED_QUARTER && NB == 128 && VB == 32)
-                node_scan_quarters(A, n, node, key, lt, valid, eq);
-            else
-                node_scan<NB, VB>(A, n, node, key, lt, valid, eq);
+            node_scan<NB, VB>(A, n, node, key, lt, valid, eq);
             uint64_t res = kIdle;
             if (eq) {
                 res = node + lt;
@@ -723,29 +723,29 @@ learned_query_kernel(const uint64_t *__restrict__ A, const LearnedGeom G, const 
                 fl |= (lt > 0 ? kSeenLess : 0u) | (lt < valid ? kSeenGreater : 0u);
                 const uint64_t nx = node + 1 <= cmax ? (node + 1) * (B + 1) + (uint64_t)lt * B - 1 : n;
                 if (nx < n) {
-                    node = nx;
+                    cur = nx | ((uint64_t)fl << kFlagShift);
                 } else if (!(fl & kSubtree) || ((fl & kSeenLess) && (fl & kSeenGreater))) {
                     res = n;  // absent (from the root; or the subtree straddles the query)
                 } else {      // the window could not decide: plain search from the root
                     ++n_fallback;
-                    node = 0;
-                    fl = 0;
+                    cur = 0;
                 }
             }
             if (res != kIdle) {
-                __stcs(ans + qid, res);
-                node = kIdle;
+                __stcs(ans + q0 + qoff, res);
+                cur = kIdle;
             }
         }
     }
     if (stats) {
+        unsigned long long f = n_fallback, d = depth_sum;
         for (int o = 16; o > 0; o >>= 1) {
-            n_fallback += __shfl_xor_sync(0xFFFFFFFFu, n_fallback, o);
-            depth_sum += __shfl_xor_sync(0xFFFFFFFFu, depth_sum, o);
+            f += __shfl_xor_sync(0xFFFFFFFFu, f, o);
+            d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
         }
         if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&stats[0], n_fallback);
-            atomicAdd(&stats[1], depth_sum);
+            atomicAdd(&stats[0], f);
+            atomicAdd(&stats[1], d);
         }
     }
 }
@@ -933,6 +933,9 @@ int query_btree_learned(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank
     // vector node loads: b in {2, 4, 8, 16, 32} on a 16-byte aligned layout
     if (b * 8 % 16 || b * 8 > 256 || ((b * 8 / 16) & (b * 8 / 16 - 1))) return TL_ERROR_UNSUPPORTED;
     if (reinterpret_cast<uintptr_t>(A) & 15) return TL_ERROR_INVALID_VALUE;
+    // the kernel keeps a warp's query offsets in 32 bits and a node index with
+    // three flag bits in 64
+    if (n >= (1ull << 61) || q >= (1ull << 44)) return TL_ERROR_UNSUPPORTED;
     if (q == 0) return TL_SUCCESS;
     LearnedGeom G;
     G.g = make_btree_geom(n, b);
