@@ -152,6 +152,7 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
     const MvebPlan &P = prm.plan;
     const uint64_t ntiles = P.total_tiles;
     int loaded_U = -1;
+    uint32_t inv_pk[2] = {0, 0};  // this lane's entries of the unit table (see below)
     const uint32_t lane = threadIdx.x & 31;
     // The next ticket is claimed as the tile ends, not as it starts: a tile's
     // stores wait for the tiles just right of it, claimed just before it, and a
@@ -166,7 +167,17 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
         const MvebRegion &R = P.reg[ri];
         if ((int)R.U != loaded_U && R.U) {  // block-uniform: unit tables for this height
             const unsigned char *src = prm.inv + unit_table_off(R.U);
+            __syncthreads();  // every lane has its packed entries of the previous table
             for (uint32_t q = threadIdx.x; q < (1u << R.U) - 1; q += blockDim.x) s_inv[q] = src[q];
+            __syncthreads();
+            // each lane's entries q = lane + 32 j (j < 8), four per register
+            inv_pk[0] = inv_pk[1] = 0;
+            const uint32_t uu = (1u << R.U) - 1;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t q = lane + 32u * j;
+                if (q < uu) inv_pk[j >> 2] |= (uint32_t)s_inv[q] << (8 * (j & 3));
+            }
             loaded_U = R.U;
         }
         if (threadIdx.x == 0) s_ok = 1;  // the previous tile's readers are past the ticket barrier
@@ -203,7 +214,11 @@ mveb_stream_kernel(K *__restrict__ A, K *__restrict__ scr, const __grid_constant
                 const uint64_t gi = gb + (uint64_t)j * nwarps;
                 const uint64_t dst = __shfl_sync(0xFFFFFFFFu, my_dst, j);
                 const uint32_t gsrc = (uint32_t)(R.src + (gi << U) - base);
-                for (uint32_t q = lane; q < u; q += 32) A[dst + q] = sm[gsrc + s_inv[q]];
+                K *d = A + dst + lane;
+                const K *g = sm + gsrc;
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj)
+                    if (lane + 32u * jj < (uint32_t)u) d[32 * jj] = g[(inv_pk[jj >> 2] >> (8 * (jj & 3))) & 0xFFu];
                 if (lane == 0 && R.src + (gi << U) + u < R.src + R.len)
                     scr[R.slot_base + gi] = sm[gsrc + u];
             }
