@@ -379,8 +379,11 @@ int tl_debug_stream_blocks_per_sm(int layout, uint32_t key_bytes);
  * schedule applies to on it, whatever it saves; 0 restores the default. */
 int tl_debug_set_schedule(int mode);
 /* Measurement hook, query kernels: 0 the default; 2 B-tree nodes in 16-byte
- * loads instead of 32-byte ones; 3 / 4 vEB two / four descents per thread in
- * lock-step; 5 B-tree top levels pinned in shared memory. */
+ * loads by a thread per query; 3 / 4 vEB two / four descents per thread in
+ * lock-step; 5 B-tree a thread per query with 32-byte loads and the top levels
+ * pinned in shared memory; 6 B-tree a thread per query with 32-byte loads (in
+ * place of a group of lanes per node, for the learned query too); 7 B-tree one
+ * 32-byte load per lane of the group (b * w / 32 lanes). */
 void tl_debug_set_query_variant(int v);
 /* Instances of a batched plan on the ordered-tile schedule and their keys: by
  * default those of 64 tiles or more (at the plan's tile size for their size

@@ -117,3 +117,30 @@ def test_btree_queries_every_node_width(b):
             Q = data.queries_np(keys, 10_000, 0.5, b)
             Q = np.concatenate([Q, keys[:1] - 1 if keys[0] > 0 else keys[:1], keys[-1:] + 1]).astype(dtype)
             assert np.array_equal(gpu_answers("btree", tree, Q, b), O.search("btree", tree, Q, b)), (b, n, dtype)
+
+
+@pytest.mark.parametrize("variant", [0, 2, 5, 6])
+def test_btree_query_kernel_forms(variant):
+    """Each B-tree node-read form gives the oracle's answers: a group of
+    b*w/32 lanes with one 32-byte load each (the default for 64-, 128- and
+    256-byte nodes), a thread per query with 32-byte loads (variant 6, and with
+    the top levels in shared memory, 5) and with 16-byte loads (2); the partial
+    last leaf and queries past both ends included."""
+    import ctypes as C
+    L = T.lib()
+    L.tl_debug_set_query_variant.argtypes = [C.c_int]
+    L.tl_debug_set_query_variant(variant)
+    try:
+        for b, dtype in [(4, np.uint64), (8, np.uint64), (16, np.uint64), (32, np.uint64), (8, np.uint32),
+                         (16, np.uint32), (32, np.uint32), (64, np.uint32)]:
+            for n in [1, b - 1, b, b + 1, 7 * b + 5, 65_537, 1_000_003]:
+                if n < 1:
+                    continue
+                keys = data.sorted_keys_np(n, 1, 16 if dtype == np.uint64 else 3, n + b, dtype)
+                tree = O.permute("btree", keys, b)
+                Q = data.queries_np(keys, 20_000, 0.5, n + 2)
+                Q = np.concatenate([Q, keys[:1] - 1 if keys[0] > 0 else keys[:1], keys[-1:] + 1]).astype(dtype)
+                assert np.array_equal(gpu_answers("btree", tree, Q, b), O.search("btree", tree, Q, b)), \
+                    (variant, b, n, dtype)
+    finally:
+        L.tl_debug_set_query_variant(0)

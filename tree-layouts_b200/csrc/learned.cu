@@ -18,6 +18,7 @@
 #include <cstddef>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "geometry.cuh"
@@ -115,9 +116,48 @@ static void compile_root(const tl_rank_model &m, RootPieces &rp) {
     }
 }
 
+static void model_to_flat(const tl_rank_model &m, float *w);
+
+// Compiled roots of the last few models seen, keyed by their root weights:
+// compiling (host, double precision, up to 33 x 33 pieces) costs more than a
+// small query batch, and one model serves many batches.
+struct RootCacheEntry {
+    float w[kParams];  // the weights the pieces were compiled from
+    RootPieces rp;
+    uint64_t stamp;
+};
+constexpr size_t kRootCacheEntries = 4;
+static std::mutex g_root_mu;
+static std::vector<std::unique_ptr<RootCacheEntry>> g_root_cache;
+static uint64_t g_root_clock = 0;
+
+static void compiled_root(const tl_rank_model &m, RootPieces &out) {
+    float w[kParams];
+    model_to_flat(m, w);
+    std::lock_guard<std::mutex> lock(g_root_mu);
+    RootCacheEntry *hit = nullptr;
+    for (auto &e : g_root_cache)
+        if (!std::memcmp(e->w, w, sizeof w)) hit = e.get();
+    if (!hit) {
+        std::unique_ptr<RootCacheEntry> e(new RootCacheEntry);
+        std::memcpy(e->w, w, sizeof w);
+        compile_root(m, e->rp);
+        if (g_root_cache.size() >= kRootCacheEntries) {
+            size_t old = 0;
+            for (size_t k = 1; k < g_root_cache.size(); ++k)
+                if (g_root_cache[k]->stamp < g_root_cache[old]->stamp) old = k;
+            g_root_cache.erase(g_root_cache.begin() + (long)old);
+        }
+        hit = e.get();
+        g_root_cache.push_back(std::move(e));
+    }
+    hit->stamp = ++g_root_clock;
+    out = hit->rp;
+}
+
 static ModelParams to_params(const tl_rank_model &m) {
     ModelParams p;
-    compile_root(m, p.root);
+    compiled_root(m, p.root);
     p.x_lo = (float)m.x_lo;
     p.x_scale = (float)m.x_scale;
     p.log_feature = m.log_feature;
@@ -188,12 +228,8 @@ static_assert(sizeof(tl_rank_leaf) == 32 && offsetof(tl_rank_leaf, slope) == 16 
                   offsetof(tl_rank_leaf, eps_lo) == 20 && offsetof(tl_rank_leaf, empty) == 28,
               "load_leaf reads the segment entry as four 64-bit words");
 
-// A segment entry (32 bytes) in one load where the table is 32-byte aligned.
-__device__ __forceinline__ tl_rank_leaf load_leaf(const tl_rank_leaf *__restrict__ leaves, uint32_t l,
-                                                  bool aligned32) {
-    if (!aligned32) return leaves[l];
-    uint64_t w[4];
-    ldg32(reinterpret_cast<const uint64_t *>(leaves + l), w);
+// A segment entry from its four 64-bit words (its layout in memory).
+__device__ __forceinline__ tl_rank_leaf leaf_from_words(const uint64_t (&w)[4]) {
     tl_rank_leaf lf;
     lf.kmin = w[0];
     lf.base = w[1];
@@ -202,6 +238,15 @@ __device__ __forceinline__ tl_rank_leaf load_leaf(const tl_rank_leaf *__restrict
     lf.eps_hi = (uint32_t)w[3];
     lf.empty = (uint32_t)(w[3] >> 32);
     return lf;
+}
+
+// A segment entry (32 bytes) in one load where the table is 32-byte aligned.
+__device__ __forceinline__ tl_rank_leaf load_leaf(const tl_rank_leaf *__restrict__ leaves, uint32_t l,
+                                                  bool aligned32) {
+    if (!aligned32) return leaves[l];
+    uint64_t w[4];
+    ldg32(reinterpret_cast<const uint64_t *>(leaves + l), w);
+    return leaf_from_words(w);
 }
 
 // Rank prediction of a segment, clamped to [0, n).
@@ -490,6 +535,7 @@ __global__ void rmi_predict_kernel(const __grid_constant__ ModelParams p, bool u
 struct LearnedGeom {
     BtreeGeom g;
     FastDiv64 fd;
+    uint64_t cmax;  // (n + 1) / (b + 1): nodes below it have a child inside the layout
 };
 
 // In-order "gap" coordinates: the top tree's ni keys split the key space into
@@ -551,46 +597,23 @@ __device__ __forceinline__ void node_scan(const uint64_t *__restrict__ A, uint64
     }
 }
 
-// A 16-key node (128 bytes, 32-byte aligned): four 32-byte loads, the quarter
-// holding q's rank from the three quarter maxima, then that quarter's keys
-// only (the keys are sorted: every key of an earlier quarter is below q).
-__device__ __forceinline__ void node_scan_quarters(const uint64_t *__restrict__ A, uint64_t n, uint64_t i, uint64_t q,
-                                                   uint32_t &lt, uint32_t &valid, bool &eq) {
-    if (i + 16 > n) {
-        node_scan<128, 32>(A, n, i, q, lt, valid, eq);
-        return;
-    }
-    valid = 16;
-    uint64_t v[4][4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) ldg32(A + i + j * 4, v[j]);
-    const uint32_t c = (v[0][3] < q) + (v[1][3] < q) + (v[2][3] < q);
-    uint64_t w[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) w[e] = c == 0 ? v[0][e] : c == 1 ? v[1][e] : c == 2 ? v[2][e] : v[3][e];
-    lt = 4 * c;
-    eq = false;
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        lt += w[e] < q;
-        eq |= w[e] == q;
-    }
-}
-
 // The start of one query's descent: the deepest subtree whose in-order rank
 // range covers the model's window (flags kSubtree), or the root.
 constexpr uint32_t kSubtree = 1, kSeenLess = 2, kSeenGreater = 4;
 
+// The segment the rank model's root assigns to q.
+__device__ __forceinline__ uint32_t learned_segment(const ModelParams &p, const PiecesSmem &sp, int use_net,
+                                                    uint64_t q) {
+    return leaf_of(p, root_eval(p, sp, feature(p, q), use_net != 0));
+}
+
 template <uint64_t B>
-__device__ __forceinline__ uint64_t learned_start(const LearnedGeom &G, const ModelParams &p, const PiecesSmem &sp,
-                                                  int use_net, const tl_rank_leaf *__restrict__ leaves, bool leaves32,
-                                                  uint64_t q, uint32_t &flags, uint32_t &depth) {
+__device__ __forceinline__ uint64_t learned_start_at(const LearnedGeom &G, const tl_rank_leaf &lf, uint64_t q,
+                                                     uint32_t &flags, uint32_t &depth) {
     const BtreeGeom &g = G.g;
     const uint64_t n = g.n;
     flags = 0;
     depth = 0;
-    const uint32_t l = leaf_of(p, root_eval(p, sp, feature(p, q), use_net != 0));
-    const tl_rank_leaf lf = load_leaf(leaves, l, leaves32);
     if (lf.empty || g.h == 0) return 0;
     const uint64_t pr = leaf_predict(lf, q, n);
     const uint64_t rlo = pr > lf.eps_lo ? pr - lf.eps_lo : 0;
@@ -616,6 +639,14 @@ __device__ __forceinline__ uint64_t learned_start(const LearnedGeom &G, const Mo
     return i;
 }
 
+template <uint64_t B>
+__device__ __forceinline__ uint64_t learned_start(const LearnedGeom &G, const ModelParams &p, const PiecesSmem &sp,
+                                                  int use_net, const tl_rank_leaf *__restrict__ leaves, bool leaves32,
+                                                  uint64_t q, uint32_t &flags, uint32_t &depth) {
+    const tl_rank_leaf lf = load_leaf(leaves, learned_segment(p, sp, use_net, q), leaves32);
+    return learned_start_at<B>(G, lf, q, flags, depth);
+}
+
 constexpr uint64_t kIdle = ~0ull;
 
 // 1024-thread blocks: two per SM hold the pieces twice in shared memory (about
@@ -628,11 +659,19 @@ constexpr uint64_t kIdle = ~0ull;
 #ifndef TL_LEARNED_MIN_BLOCKS
 #define TL_LEARNED_MIN_BLOCKS 1
 #endif
-#ifndef TL_LEARNED_QUARTER
-#define TL_LEARNED_QUARTER 0
-#endif
 
 constexpr int kLearnedThreads = TL_LEARNED_THREADS;
+// The group-read kernel: 768-thread blocks, two per SM at 40 registers (no
+// spills); measured on B200 (2^28 Zipf queries over 2^30 skewed u64 keys,
+// b = 16) 16.4e9 q/s against 15.8e9 with one 1024-thread block per SM, 15.9e9
+// with two, 15.6e9 with three 512-thread blocks.
+#ifndef TL_LEARNED_GROUP_THREADS
+#define TL_LEARNED_GROUP_THREADS 768
+#endif
+#ifndef TL_LEARNED_GROUP_MIN_BLOCKS
+#define TL_LEARNED_GROUP_MIN_BLOCKS 2
+#endif
+constexpr int kLearnedGroupThreads = TL_LEARNED_GROUP_THREADS;
 
 // One descent per lane, fed from a per-warp queue: a lane whose descent ends
 // takes the next prepared query at once, so start depths that differ, hits at
@@ -751,6 +790,156 @@ learned_query_kernel(const uint64_t *__restrict__ A, const LearnedGeom G, const 
 }
 
 // ---------------------------------------------------------------- host
+// The same queue feeding a group of GL lanes per descent instead of one lane:
+// lane g reads node slots 4g + 4 GL j + [0, 4) with load j of NL = NB / (32 GL)
+// 32-byte loads, so each load instruction of a warp touches 32 / GL node lines
+// of GL sectors, one L1 wavefront each (the plain B-tree query's node read).
+// Idle groups take the prepared starts in group order; the group adds its
+// lanes' counts with full-warp shuffles and learns of an equal key by ballot.
+template <int NB, int GL, bool kStats>
+__global__ void __launch_bounds__(kLearnedGroupThreads, TL_LEARNED_GROUP_MIN_BLOCKS)
+learned_query_group_kernel(const uint64_t *__restrict__ A, const LearnedGeom G, const __grid_constant__ ModelParams p,
+                           int use_net, const tl_rank_leaf *__restrict__ leaves, const uint64_t *__restrict__ Q,
+                           uint64_t nq, uint64_t *__restrict__ ans, unsigned long long *__restrict__ stats) {
+    constexpr uint64_t B = NB / 8;
+    constexpr int KPL = 4;               // keys per 32-byte load
+    constexpr int NL = NB / (32 * GL);   // loads per lane and node
+    static_assert((GL == 2 || GL == 4 || GL == 8) && NL >= 1 && NL * GL * 32 == NB, "2, 4 or 8 lanes per node");
+    constexpr unsigned kLeaders = GL == 2 ? 0x55555555u : GL == 4 ? 0x11111111u : 0x01010101u;
+    constexpr uint64_t kFlagShift = 61, kNodeMask = (1ull << kFlagShift) - 1;
+    __shared__ PiecesSmem sp;
+    if (use_net) stage_pieces(p, sp);
+    const bool leaves32 = (reinterpret_cast<uintptr_t>(leaves) & 31) == 0;
+    const uint64_t n = G.g.n;
+    const uint64_t cmax = G.cmax;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t g = lane % GL, lead = lane - g;
+    const unsigned below = (1u << lane) - 1u, below_lead = (1u << lead) - 1u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t per = (nq + warps - 1) / warps;  // below 2^32 (the host checks q)
+    const uint64_t q0 = min(nq, w * per);
+    const uint32_t cnt = (uint32_t)(min(nq, q0 + per) - q0);
+    uint32_t n_fallback = 0, depth_sum = 0;
+    uint64_t cur = kIdle, key = 0;  // this group's descent: node | flags << kFlagShift
+    uint32_t qoff = 0;
+    uint64_t e_cur = 0, e_key = 0;  // this lane's prepared entry of the current batch
+    uint32_t next = 0, batch0 = 0, bn = 0, bpos = 0;
+    (void)below;
+    for (;;) {
+        unsigned need = __ballot_sync(0xFFFFFFFFu, cur == kIdle) & kLeaders;
+        while (need) {
+            if (bpos == bn) {
+                if (next >= cnt) break;
+                batch0 = next;
+                bn = cnt - next < 32 ? cnt - next : 32;
+                bpos = 0;
+                next += bn;
+                if (lane < bn) {
+                    e_key = __ldcs(Q + q0 + batch0 + lane);
+                    uint32_t f, d;
+                    const uint64_t nd = learned_start<B>(G, p, sp, use_net, leaves, leaves32, e_key, f, d);
+                    e_cur = nd | ((uint64_t)f << kFlagShift);
+                    if (kStats) {
+                        if (f) depth_sum += d; else ++n_fallback;
+                    }
+                }
+            }
+            const uint32_t avail = bn - bpos;
+            unsigned take = need;
+            if ((uint32_t)__popc(need) > avail) {  // the lowest `avail` idle groups
+                take = 0;
+                unsigned m = need;
+                for (uint32_t c = 0; c < avail; ++c) {
+                    const unsigned low = m & (0u - m);
+                    take |= low;
+                    m ^= low;
+                }
+            }
+            const bool mine = (take >> lead) & 1u;
+            const uint32_t src = bpos + __popc(take & below_lead);
+            const uint64_t k2 = __shfl_sync(0xFFFFFFFFu, e_key, mine ? src : 0);
+            const uint64_t c2 = __shfl_sync(0xFFFFFFFFu, e_cur, mine ? src : 0);
+            if (mine) {
+                key = k2;
+                cur = c2;
+                qoff = batch0 + src;
+            }
+            bpos += __popc(take);
+            need &= ~take;
+        }
+        if (!__any_sync(0xFFFFFFFFu, cur != kIdle)) break;
+        const bool live = cur != kIdle;
+        const uint64_t node = cur & kNodeMask;
+        uint32_t lt = 0;
+        bool eq = false;
+        if (live) {
+            const uint64_t s0 = node + (uint64_t)g * KPL;
+            if (node + B <= n) {
+                uint64_t v[NL][KPL];
+#pragma unroll
+                for (int j = 0; j < NL; ++j) ldg32(A + s0 + (uint64_t)j * GL * KPL, v[j]);
+#pragma unroll
+                for (int j = 0; j < NL; ++j)
+#pragma unroll
+                    for (int e = 0; e < KPL; ++e) {
+                        lt += v[j][e] < key;
+                        eq |= v[j][e] == key;
+                    }
+            } else {  // the partial last leaf: slots at or past n do not count
+#pragma unroll
+                for (int j = 0; j < NL; ++j)
+#pragma unroll
+                    for (int e = 0; e < KPL; ++e) {
+                        const uint64_t pos = s0 + (uint64_t)j * GL * KPL + e;
+                        if (pos < n) {
+                            const uint64_t c = __ldg(A + pos);
+                            lt += c < key;
+                            eq |= c == key;
+                        }
+                    }
+            }
+        }
+#pragma unroll
+        for (int off = GL / 2; off > 0; off >>= 1) lt += __shfl_xor_sync(0xFFFFFFFFu, lt, off);
+        const bool hit = ((__ballot_sync(0xFFFFFFFFu, eq) >> lead) & ((1u << GL) - 1)) != 0;
+        if (live) {
+            const uint32_t valid = node + B <= n ? (uint32_t)B : (uint32_t)(n - node);
+            uint32_t fl = (uint32_t)(cur >> kFlagShift);
+            uint64_t res = kIdle;
+            if (hit) {
+                res = node + lt;
+            } else {
+                fl |= (lt > 0 ? kSeenLess : 0u) | (lt < valid ? kSeenGreater : 0u);
+                const uint64_t nx = node + 1 <= cmax ? (node + 1) * (B + 1) + (uint64_t)lt * B - 1 : n;
+                if (nx < n) {
+                    cur = nx | ((uint64_t)fl << kFlagShift);
+                } else if (!(fl & kSubtree) || ((fl & kSeenLess) && (fl & kSeenGreater))) {
+                    res = n;  // absent (from the root; or the subtree straddles the query)
+                } else {      // the window could not decide: plain search from the root
+                    if (kStats && g == 0) ++n_fallback;
+                    cur = 0;
+                }
+            }
+            if (res != kIdle) {
+                if (g == 0) __stcs(ans + q0 + qoff, res);
+                cur = kIdle;
+            }
+        }
+    }
+    if (kStats && stats) {
+        unsigned long long f = n_fallback, d = depth_sum;
+        for (int o = 16; o > 0; o >>= 1) {
+            f += __shfl_xor_sync(0xFFFFFFFFu, f, o);
+            d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&stats[0], f);
+            atomicAdd(&stats[1], d);
+        }
+    }
+}
+
 static void init_model(tl_rank_model &m, const tl_rank_train_config &cfg) {
     memset(&m, 0, sizeof m);
     // layer 1: ramps with breakpoints spread over [0, 1]
@@ -940,34 +1129,56 @@ int query_btree_learned(const uint64_t *A, uint64_t n, uint64_t b, const tl_rank
     LearnedGeom G;
     G.g = make_btree_geom(n, b);
     G.fd = FastDiv64(b + 1);
+    G.cmax = (n + 1) / (b + 1);
     EventTimer timer(ms != nullptr, st);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    timer.start();
     const ModelParams p = to_params(*m);
     const int use_net = m->train_root != 0;
-    auto launch = [&](auto kern) -> int {
+    auto launch_with = [&](auto kern, int threads) -> int {
         // the smallest shared-memory carve-out that holds the blocks' pieces:
         // the rest stays L1
         TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 15));
         int per_sm = 0;
-        TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLearnedThreads, 0));
-        uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms,
-                                           (q + kLearnedThreads - 1) / kLearnedThreads);
-        kern<<<(unsigned)std::max<uint64_t>(grid, 1), kLearnedThreads, 0, st>>>(A, G, p, use_net, leaves, Q, q, ans,
-                                                                               stats);
+        TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
+        uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, (q + threads - 1) / threads);
+        timer.start();
+        kern<<<(unsigned)std::max<uint64_t>(grid, 1), threads, 0, st>>>(A, G, p, use_net, leaves, Q, q, ans, stats);
         return TL_SUCCESS;
     };
-    // 32-byte node loads on a 32-byte aligned layout (node bytes a multiple of 32), else 16-byte ones
+    auto launch = [&](auto kern) -> int { return launch_with(kern, kLearnedThreads); };
+    auto launch_group = [&](auto kern) -> int { return launch_with(kern, kLearnedGroupThreads); };
+    // 64-, 128- and 256-byte nodes on a 32-byte aligned layout: a group of
+    // lanes per descent; else one lane per descent with 32-byte node loads
+    // (32-byte aligned layout, node bytes a multiple of 32) or 16-byte ones
     const bool v32 = (reinterpret_cast<uintptr_t>(A) & 31) == 0 && (b * 8) % 32 == 0;
+    const bool grp = v32 && query_variant() != 6;
     int rc;
     switch (b * 8) {
         case 16: rc = launch(learned_query_kernel<16, 16>); break;
         case 32: rc = v32 ? launch(learned_query_kernel<32, 32>) : launch(learned_query_kernel<32, 16>); break;
-        case 64: rc = v32 ? launch(learned_query_kernel<64, 32>) : launch(learned_query_kernel<64, 16>); break;
-        case 128: rc = v32 ? launch(learned_query_kernel<128, 32>) : launch(learned_query_kernel<128, 16>); break;
-        case 256: rc = v32 ? launch(learned_query_kernel<256, 32>) : launch(learned_query_kernel<256, 16>); break;
+        case 64:
+            rc = grp   ? (stats ? launch_group(learned_query_group_kernel<64, 2, true>)
+                                : launch_group(learned_query_group_kernel<64, 2, false>))
+                 : v32 ? launch(learned_query_kernel<64, 32>)
+                       : launch(learned_query_kernel<64, 16>);
+            break;
+        case 128:
+            rc = grp && query_variant() == 7
+                     ? (stats ? launch_group(learned_query_group_kernel<128, 4, true>)
+                              : launch_group(learned_query_group_kernel<128, 4, false>))
+                 : grp   ? (stats ? launch_group(learned_query_group_kernel<128, 2, true>)
+                                  : launch_group(learned_query_group_kernel<128, 2, false>))
+                 : v32 ? launch(learned_query_kernel<128, 32>)
+                       : launch(learned_query_kernel<128, 16>);
+            break;
+        case 256:
+            rc = grp   ? (stats ? launch_group(learned_query_group_kernel<256, 4, true>)
+                                : launch_group(learned_query_group_kernel<256, 4, false>))
+                 : v32 ? launch(learned_query_kernel<256, 32>)
+                       : launch(learned_query_kernel<256, 16>);
+            break;
         default: return TL_ERROR_UNSUPPORTED;
     }
     if (rc) return rc;

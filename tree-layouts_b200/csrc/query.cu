@@ -292,6 +292,87 @@ btree_query_v32_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, const K 
     }
 }
 
+// G lanes per query read a node together with NL = NB / (32 G) 32-byte loads
+// each (lane g holds slots g * KPL + j * G * KPL + [0, KPL) for load j).  Each
+// load instruction of a warp then touches 32 / G node lines with G sectors of
+// a line in one L1 wavefront, where a thread per query spends a wavefront per
+// sector; fewer lanes per node keep more descents in flight.  Control flow is
+// warp-uniform (a warp takes 32 / G queries per round and descends while any of
+// them is live), so the group's count is a full-warp shuffle sum and an equal
+// key in any of its lanes, found by ballot, ends its descent.  (Descending to
+// the last level on counts alone and checking q's successor with one load at
+// the end measured 9 % slower on B200: that load adds a dependent step to every
+// warp's round.)
+template <typename K, int NB, int G>
+__global__ void __launch_bounds__(kQueryThreads)
+btree_query_group32_kernel(const K *__restrict__ A, uint64_t n, const K *__restrict__ Q, uint64_t nq,
+                           uint64_t *__restrict__ ans) {
+    constexpr int KPL = 32 / sizeof(K);  // keys per 32-byte load
+    constexpr int NL = NB / 32 / G;      // 32-byte loads per lane and node
+    constexpr int B = NB / sizeof(K);    // == b
+    constexpr int QPW = 32 / G;          // queries per warp and round
+    static_assert(G >= 2 && G <= 8 && (G & (G - 1)) == 0 && NL >= 1 && NL * G * 32 == NB,
+                  "group of 2, 4 or 8 lanes");
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t g = lane % G;
+    const uint32_t gshift = lane - g;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const uint64_t cmax = (n + 1) / (B + 1);
+    for (uint64_t base = wid * QPW; base < nq; base += warps * QPW) {
+        const uint64_t qi = base + lane / G;
+        bool live = qi < nq && n > 0;
+        const K q = qi < nq ? __ldcs(Q + qi) : K(0);
+        uint64_t i = 0, res = n;
+        while (__any_sync(0xFFFFFFFFu, live)) {
+            uint32_t lt = 0;
+            bool eq = false;
+            if (live) {
+                const uint64_t s0 = i + (uint64_t)g * KPL;  // lane g: slots s0 + j * G * KPL + e
+                if (i + B <= n) {
+                    K v[NL][KPL];
+#pragma unroll
+                    for (int j = 0; j < NL; ++j) ldg32(A + s0 + (uint64_t)j * G * KPL, v[j]);
+#pragma unroll
+                    for (int j = 0; j < NL; ++j)
+#pragma unroll
+                        for (int e = 0; e < KPL; ++e) {
+                            lt += v[j][e] < q;
+                            eq |= v[j][e] == q;
+                        }
+                } else {  // the partial last leaf: slots at or past n do not count
+#pragma unroll
+                    for (int j = 0; j < NL; ++j)
+#pragma unroll
+                        for (int e = 0; e < KPL; ++e) {
+                            const uint64_t p = s0 + (uint64_t)j * G * KPL + e;
+                            if (p < n) {
+                                const K cur = __ldg(A + p);
+                                lt += cur < q;
+                                eq |= cur == q;
+                            }
+                        }
+                }
+            }
+#pragma unroll
+            for (int off = G / 2; off > 0; off >>= 1) lt += __shfl_xor_sync(0xFFFFFFFFu, lt, off);
+            const bool hit = ((__ballot_sync(0xFFFFFFFFu, eq) >> gshift) & ((1u << G) - 1)) != 0;
+            if (live) {
+                if (hit) {
+                    res = i + lt;
+                    live = false;
+                } else if (i + 1 > cmax) {
+                    live = false;
+                } else {
+                    i = (i + 1) * (B + 1) + (uint64_t)lt * B - 1;
+                    live = i < n;
+                }
+            }
+        }
+        if (g == 0 && qi < nq) __stcs(ans + qi, res);
+    }
+}
+
 static int g_query_variant = 0;
 void set_query_variant(int v) { g_query_variant = v; }
 int query_variant() { return g_query_variant; }
@@ -478,9 +559,11 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
         }
         P = std::min<uint64_t>(top, a.n);
         size_t smem = P * sizeof(K);
-        // a thread per query with 32-byte node loads (b * w a multiple of 32 on
-        // a 32-byte aligned layout), else 16-byte ones (b * w a multiple of
-        // 16), else a group of lanes per query with one key per lane
+        // a group of max(2, b * w / 64) lanes per query with 32-byte loads (b * w
+        // = 64, 128 or 256 on a 32-byte aligned layout), else a thread per query
+        // with 32-byte node loads (b * w a multiple of 32), else 16-byte ones
+        // (b * w a multiple of 16), else a group of lanes per query with one key
+        // per lane
         const uint64_t node_bytes = a.b * sizeof(K);
         const uintptr_t base = reinterpret_cast<uintptr_t>(A);
         int rc = TL_SUCCESS;
@@ -500,7 +583,38 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
             return TL_SUCCESS;
         };
         const bool pin = g_query_variant == 5;
-        if ((base & 31) == 0 && node_bytes % 32 == 0 && g_query_variant != 2) {
+        auto grp = [&](auto kern, uint64_t lanes_per_query) -> int {
+            rc = persistent_grid(kern, 0, a.q * lanes_per_query, &grid);
+            if (rc) return rc;
+            kern<<<grid, kQueryThreads, 0, st>>>(A, a.n, Q, a.q, a.answers);
+            done = true;
+            return TL_SUCCESS;
+        };
+        // default: nodes of 64, 128 or 256 bytes on a 32-byte aligned layout are
+        // read by a group of max(2, node_bytes / 64) lanes.  Measured on B200,
+        // 2^27 queries, q/s with 2 / 4 / 8 lanes per node against a thread per
+        // query with 32-byte loads: b = 16 u64 over 5e8 keys 14.2e9 / 9.53e9 /
+        // - against 6.54e9; b = 32 u64 over 2^28 keys 8.33e9 / 9.08e9 / 6.06e9
+        // against 4.28e9; b = 16 u32 over 2^30 keys 17.7e9 against 11.7e9;
+        // b = 8 u64 over 2^30 keys 12.7e9 against 8.56e9
+        if ((base & 31) == 0 && g_query_variant != 2 && g_query_variant != 5 && g_query_variant != 6) {
+            if (g_query_variant == 7) {  // one 32-byte load per lane
+                switch (node_bytes) {
+                    case 128: rc = grp(btree_query_group32_kernel<K, 128, 4>, 4); break;
+                    case 256: rc = grp(btree_query_group32_kernel<K, 256, 8>, 8); break;
+                    default: break;
+                }
+            }
+            if (!done) {  // two 32-byte loads per lane (one for 64-byte nodes)
+                switch (node_bytes) {
+                    case 64: rc = grp(btree_query_group32_kernel<K, 64, 2>, 2); break;
+                    case 128: rc = grp(btree_query_group32_kernel<K, 128, 2>, 2); break;
+                    case 256: rc = grp(btree_query_group32_kernel<K, 256, 4>, 4); break;
+                    default: break;
+                }
+            }
+        }
+        if (!done && (base & 31) == 0 && node_bytes % 32 == 0 && g_query_variant != 2) {
             switch (node_bytes) {
                 case 32: rc = pin ? v32(btree_query_v32_kernel<K, 32, true>, true) : v32(btree_query_v32_kernel<K, 32, false>, false); break;
                 case 64: rc = pin ? v32(btree_query_v32_kernel<K, 64, true>, true) : v32(btree_query_v32_kernel<K, 64, false>, false); break;
