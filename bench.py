@@ -99,6 +99,23 @@ def query_bytes_model(layout, n, b, kb):
     return kb + 8 + fetch * (len(sizes) - l2_levels), l2_levels, len(sizes)
 
 
+def query_kernel_name(layout, b, kb):
+    """The kernel the library launches for a query batch over a 32-byte aligned
+    layout (torch allocations are)."""
+    if layout == "btree":
+        nb = b * kb
+        if nb in (64, 128, 256):
+            return f"btree_query_group32_kernel ({max(2, nb // 64)} lanes per node, 32-byte loads)"
+        if nb % 32 == 0 and nb <= 256:
+            return "btree_query_v32_kernel (a thread per query, 32-byte loads)"
+        if nb % 16 == 0 and nb <= 256:
+            return "btree_query_vec_kernel (a thread per query, 16-byte loads)"
+        return "btree_query_kernel (a lane per key)"
+    if layout == "bst":
+        return "bst_query_kernel"
+    return "veb_query_kernel"
+
+
 def dist_setup(n_gpus):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -335,6 +352,9 @@ def learned_section(args, dev):
            "n": n, "q": q, "plain_queries_per_s": round(q / (pm * 1e-3), 1),
            "learned_queries_per_s": round(q / (lm * 1e-3), 1), "speedup": round(pm / lm, 3),
            "exact": exact, "plain_ms": round(pm, 3), "learned_ms": round(lm, 3),
+           "kernels": {"plain": query_kernel_name("btree", b, 8),
+                       "learned": "learned_query_group_kernel (2 lanes per node, a per-warp queue of "
+                                  "prepared starts)"},
            "fallback_frac": round(int(stats[0].item()) / q, 4),
            "mean_start_depth": round(int(stats[1].item()) / q, 3),
            "train_ms": round(train_ms, 1), "train_loss": model.train_loss, "keygen_s": round(gen_s, 1),
@@ -676,7 +696,7 @@ def run_ours(args, rank, world, local):
                               "roofline_queries_per_s": round(peak * 1e9 / qbytes, 1),
                               "frac": round(qps * qbytes / (peak * 1e9), 4),
                               "model": "w + 8 + one node fetch per level below the L2-resident depth"},
-                 "hits": hits, "kernel": f"plain {layout} query",
+                 "hits": hits, "kernel": query_kernel_name(layout, b or 16, kb),
                  "binary_search_queries_per_s": round(q / (sms * 1e-3), 1),
                  "binary_search_hits": int((sans != n).sum().item())}
         if host_layout is not None:
