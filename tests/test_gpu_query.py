@@ -144,3 +144,72 @@ def test_btree_query_kernel_forms(variant):
                     (variant, b, n, dtype)
     finally:
         L.tl_debug_set_query_variant(0)
+
+
+@pytest.mark.parametrize("variant", [0, 3, 4])
+@pytest.mark.parametrize("layout", ["mveb", "veb"])
+def test_veb_query_kernel_forms(variant, layout):
+    """Each vEB descent form gives the oracle's answers, perfect and
+    non-perfect trees, u32 and u64: one descent per thread (default), two or
+    four in lock-step (3, 4)."""
+    import ctypes as C
+    L = T.lib()
+    L.tl_debug_set_query_variant.argtypes = [C.c_int]
+    L.tl_debug_set_query_variant(variant)
+    try:
+        for dtype in (np.uint32, np.uint64):
+            for n in [1, 2, 3, 7, 100, 4095, 65536, 1_000_003, 2**21 - 1]:
+                keys = data.sorted_keys_np(n, 1, 3, n + 11, dtype)
+                tree = O.permute(layout, keys, 16)
+                Q = data.queries_np(keys, 20_000, 0.5, n + 12)
+                Q = np.concatenate([Q, keys[:1] - 1 if keys[0] > 0 else keys[:1], keys[-1:] + 1]).astype(dtype)
+                assert np.array_equal(gpu_answers(layout, tree, Q), O.search(layout, tree, Q, 16)), \
+                    (variant, layout, n, dtype)
+    finally:
+        L.tl_debug_set_query_variant(0)
+
+
+@pytest.mark.parametrize("layout,n,kb", [("mveb", 2**24 - 1, 4), ("mveb", 20_000_003, 4), ("veb", 2**22 - 1, 8),
+                                         ("bst", 2**23 - 1, 8), ("bst", 9_000_001, 4)])
+def test_partitioned_queries_match_unpartitioned(layout, n, kb):
+    """A batch searched grouped by value (a four-pass partition of the batch's
+    value range into 65536 buckets, answers written back through the carried
+    index; variant 20 forces it at any size) equals the batch searched as
+    given (variant 19) for batch lengths around the partition's 4096-entry
+    tiles, with duplicates and a batch of one value; every hit names its key's
+    slot and every miss is a key absent from the sorted keys."""
+    import ctypes as C
+
+    import torch
+    L = T.lib()
+    L.tl_debug_set_query_variant.argtypes = [C.c_int]
+    keys = data.sorted_keys_torch(n, 1, 3 if kb == 4 else 16, n % 1000 + 1, kb)
+    tree = keys.clone()
+    T.permute(layout, tree, 16)
+    tabs = T.VebTablesDevice(n, "cuda", standard=layout == "veb") if layout != "bst" else None
+    Qall = data.queries_torch(keys, 2**21, 0.5, 7)
+    Qall[:3] = keys[0]  # duplicates and the smallest key
+    for q in [1, 2, 4095, 4096, 4097, 100_003, 2**21]:
+        Q = Qall[:q].clone()
+        got = torch.empty(q, dtype=torch.int64, device="cuda")
+        exp = torch.empty_like(got)
+        try:
+            L.tl_debug_set_query_variant(20)
+            T.query(layout, tree, Q, got, 16, tables=tabs)
+            L.tl_debug_set_query_variant(19)
+            T.query(layout, tree, Q, exp, 16, tables=tabs)
+        finally:
+            L.tl_debug_set_query_variant(0)
+        assert torch.equal(got, exp), (layout, n, q)
+        hit = got != n
+        assert torch.equal(tree[got[hit]], Q[hit])
+        pos = torch.searchsorted(keys, Q).clamp_max(n - 1)
+        assert torch.equal(keys[pos] == Q, hit)
+    Q = torch.full((5000,), int(keys[n // 2].item()), dtype=keys.dtype, device="cuda")  # one value
+    got = torch.empty(5000, dtype=torch.int64, device="cuda")
+    try:
+        L.tl_debug_set_query_variant(20)
+        T.query(layout, tree, Q, got, 16, tables=tabs)
+    finally:
+        L.tl_debug_set_query_variant(0)
+    assert torch.equal(tree[got], Q)
