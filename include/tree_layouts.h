@@ -79,8 +79,11 @@ int tl_permute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_
                                uint64_t *bytes);
 
 /* Generic in-place permutation sorted -> layout.  key_bytes is 4 or 8.
- * dev_workspace may be NULL: the library then allocates it stream-ordered
- * (cudaMallocAsync) and frees it before returning.
+ * dev_workspace may be NULL: the library then takes a device buffer from a
+ * small per-device cache that it fills with cudaMalloc (at most 8 buffers,
+ * kept for the life of the process, each lent to one call at a time; when no
+ * cached buffer can be had, a stream-ordered cudaMallocAsync that the call
+ * frees before returning).
  * Per-geometry tables: a B-tree or BST of 64 tiles or more (16384 for the BST)
  * takes the ordered-tile schedule, whose tables depend only on (n, b, tile
  * size).  The first call for a new geometry on a device builds them and copies
@@ -156,8 +159,8 @@ int tl_permute_algorithm(int layout, int algorithm, void *dev_A, uint64_t n, uin
  * same layout, b and key width) back to sorted order, in place.  No counterpart
  * in the reference, whose README describes conversions between sorted order and
  * the layouts but implements only sorted -> layout.  Workspace, stream and ms
- * as for tl_permute (dev_workspace NULL: stream-ordered allocation of
- * tl_unpermute_workspace_bytes, a copy of the array). */
+ * as for tl_permute (dev_workspace NULL: a cached buffer of
+ * tl_unpermute_workspace_bytes, which holds a copy of the array). */
 int tl_unpermute_workspace_bytes(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *bytes);
 int tl_unpermute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes, void *dev_workspace,
                  uint64_t workspace_bytes, void *stream, float *ms);

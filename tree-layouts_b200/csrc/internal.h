@@ -81,6 +81,11 @@ class EventTimer {
 
 // Reads a device word written by the preceding work on `st` (blocks the host).
 int read_error_word(const unsigned int *dev_word, unsigned int *out, cudaStream_t st);
+// A cached device buffer of at least `bytes` for one synchronous call (nullptr
+// when none can be had); give it back with workspace_release once the call's
+// work on its stream has finished.
+void *workspace_acquire(size_t bytes);
+void workspace_release(void *p);
 int sync_and_check(cudaStream_t st);
 struct Ctrl;
 // Keeps the wait statistics of a permutation's control block (tl_debug_wait_stats).

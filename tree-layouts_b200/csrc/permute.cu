@@ -573,13 +573,19 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
     EventTimer timer(ms != nullptr || phase_ms != nullptr, st);
     char *ws = static_cast<char *>(dev_ws);
     bool owned = false;
+    bool pooled = false;
     if (!ws) {
-        keep_pool_memory();
-        if (cudaMallocAsync(reinterpret_cast<void **>(&ws), pl.bytes, st) != cudaSuccess) {
-            record_cuda_error(cudaGetLastError());
-            return TL_ERROR_OUT_OF_MEMORY;
+        ws = static_cast<char *>(workspace_acquire(pl.bytes));
+        if (ws) {
+            owned = true;
+        } else {  // the cache could not help: a stream-ordered allocation
+            keep_pool_memory();
+            if (cudaMallocAsync(reinterpret_cast<void **>(&ws), pl.bytes, st) != cudaSuccess) {
+                record_cuda_error(cudaGetLastError());
+                return TL_ERROR_OUT_OF_MEMORY;
+            }
+            owned = pooled = true;
         }
-        owned = true;
     }
     timer.start();
     rc = key_bytes == 8 ? launch_permute<uint64_t>(pl, static_cast<uint64_t *>(dev_A), ws, st, timer)
@@ -591,8 +597,12 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
         rc = read_error_word(&ctrl->error, &err, st);
         if (rc == TL_SUCCESS) record_wait_stats(ctrl, st);
     }
-    if (owned) cudaFreeAsync(ws, st);
+    if (owned && pooled) cudaFreeAsync(ws, st);
     if (rc == TL_SUCCESS) rc = sync_and_check(st);
+    if (owned && !pooled) {
+        if (rc != TL_SUCCESS) cudaStreamSynchronize(st);  // nothing of this call may still use it
+        workspace_release(ws);
+    }
     // a bounded wait expired, or (never expected) the ordered schedule found a
     // scratch store without scratch and skipped it
     if (rc == TL_SUCCESS && err) rc = (err & (1u << TL_ERROR_TIMEOUT)) ? TL_ERROR_TIMEOUT : TL_ERROR_UNSUPPORTED;

@@ -5,8 +5,9 @@
 // allowed, e.g. a plugin inside a host engine that owns every device
 // allocation and hands out fixed memory budgets, or a latency-critical service
 // that must not hit cudaMalloc's implicit device synchronisation or its
-// failure modes in the middle of a request.  tl_permute either allocates its
-// workspace (cudaMallocAsync) or takes one from the caller; this entry point
+// failure modes in the middle of a request.  tl_permute either takes its
+// workspace from the library's buffer cache (filled by cudaMalloc) or from the
+// caller; this entry point
 // does neither: its workspace is the fixed array below, which lives in the
 // library's device image.
 //

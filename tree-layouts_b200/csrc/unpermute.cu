@@ -234,12 +234,18 @@ int unpermute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_byte
     EventTimer timer(ms != nullptr, st);
     char *ws = static_cast<char *>(dev_ws);
     bool owned = false;
+    bool pooled = false;
     if (!ws) {
-        if (cudaMallocAsync(reinterpret_cast<void **>(&ws), need, st) != cudaSuccess) {
-            record_cuda_error(cudaGetLastError());
-            return TL_ERROR_OUT_OF_MEMORY;
+        ws = static_cast<char *>(workspace_acquire(need));
+        if (ws) {
+            owned = true;
+        } else {  // the cache could not help: a stream-ordered allocation
+            if (cudaMallocAsync(reinterpret_cast<void **>(&ws), need, st) != cudaSuccess) {
+                record_cuda_error(cudaGetLastError());
+                return TL_ERROR_OUT_OF_MEMORY;
+            }
+            owned = pooled = true;
         }
-        owned = true;
     }
     timer.start();
     rc = TL_SUCCESS;
@@ -253,8 +259,12 @@ int unpermute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_byte
                             : launch_unpermute<uint32_t>(geo, static_cast<uint32_t *>(dev_A),
                                                          reinterpret_cast<const uint32_t *>(ws), st);
     timer.stop();
-    if (owned) cudaFreeAsync(ws, st);
+    if (owned && pooled) cudaFreeAsync(ws, st);
     if (rc == TL_SUCCESS) rc = sync_and_check(st);
+    if (owned && !pooled) {
+        if (rc != TL_SUCCESS) cudaStreamSynchronize(st);  // nothing of this call may still use it
+        workspace_release(ws);
+    }
     if (rc == TL_SUCCESS && ms) *ms = timer.elapsed();
     return rc;
 }
