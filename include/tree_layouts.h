@@ -408,6 +408,12 @@ int tl_debug_wait_stats(uint64_t *stalled_waits, uint64_t *polls);
 /* Keys the permutation of (layout, n, b, key_bytes) moves through its scratch
  * buffer (the second pass reads and writes each once). */
 int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
+/* The ordered-tile tables of (layout, n, b, key_bytes) computed on the host and
+ * with their per-tile passes as kernels on `stream` (what a permutation does
+ * for a geometry not seen before), uncached, compared entry by entry: 1 equal,
+ * 0 different, a negative status when the geometry has no such tables or the
+ * kernels could not run. */
+int tl_debug_order_tables_match(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, void *stream);
 /* tl_permute with library-allocated workspace, reporting the device time of its
  * two passes: phase_ms[0] = setup + stream kernel, phase_ms[1] = the second pass
  * (B-tree: scratch copy kernel, or the fix kernel of the ordered schedule;

@@ -122,3 +122,20 @@ def _full_size_properties(layout, b, n, key_bytes, gap):
 ])
 def test_full_size_properties(layout, b, n, kb, gap):
     _full_size_properties(layout, b, n, kb, gap)
+
+
+@pytest.mark.parametrize("layout,b,n,kb", [("btree", 16, 500_000_000, 8), ("btree", 16, 2**30, 8),
+                                           ("btree", 8, 60_000_000, 8), ("btree", 3, 20_000_000, 8),
+                                           ("btree", 2, 9_999_991, 4), ("btree", 17, 123_456_789, 8),
+                                           ("btree", 32, 2**27, 4), ("bst", 1, 2**30 - 1, 8),
+                                           ("bst", 1, 2**26 + 12345, 4), ("btree", 16, 2**20 + 7, 8)])
+def test_ordered_tables_gpu_build_equals_host_build(layout, b, n, kb):
+    """A permutation of a geometry not seen before computes its ordered-tile
+    tables with two kernels (each tile's predecessor, each tile's scratch count
+    under both tie orders) and the chain walk on the host; the result is the
+    host build's, entry by entry (tickets, scratch slots, bulk ranges, fix
+    segments)."""
+    import ctypes as C
+    L = T.lib()
+    L.tl_debug_order_tables_match.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]
+    assert L.tl_debug_order_tables_match(T.LAYOUTS[layout], n, b, kb, None) == 1, (layout, b, n, kb)

@@ -15,12 +15,15 @@
 // at 2^30 keys, 10 % of a b = 8 tree of 6e7 keys and 20 % of a BST of 2^30 - 1
 // keys for the second pass.
 //
-// The tables depend on (n, b, tile_keys) only.  They are computed once on the
-// host (O(tiles): a few source runs per tile; the per-tile passes and the two
-// tie orders on the host's threads) and copied once to each device
-// that uses them; both copies live until the process exits.  A geometry seen
-// for the first time while its stream is being captured gets no device copy
-// (the permutation then takes plan R or L).
+// The tables depend on (n, b, tile_keys) only.  They are computed once per
+// process (O(tiles): a few source runs per tile) and copied once to each device
+// that uses them.  A permutation computes them with its two per-tile passes as
+// kernels on its own stream (btree_order_prepare; the BST of 2^30 - 1 keys
+// took 115 ms with them on 8 host threads); other callers, and a permutation
+// whose kernels cannot run, compute them on the host's threads.  Host and
+// device copies live until the process exits.  A geometry seen for the first
+// time while its stream is being captured gets no device copy (the permutation
+// then takes plan R or L).
 #include <algorithm>
 #include <memory>
 #include <mutex>
@@ -62,41 +65,97 @@ static void order_preds(const BtreeStream &S, std::vector<int64_t> &pred) {
     parallel_tiles(N, [&](uint64_t u0, uint64_t u1) { order_preds_range(S, pred, u0, u1); });
 }
 
-static void order_preds_range(const BtreeStream &S, std::vector<int64_t> &pred, uint64_t u0, uint64_t u1) {
+// pred(u): the source tile with the longest run into tile u, if that run holds
+// at least tile_keys / 8 keys, else -1.
+TL_HD int64_t order_pred_of(const BtreeStream &S, uint64_t u) {
     const uint64_t T = S.tile_keys, thr = T / 8;
-    for (uint64_t u = u0; u < u1; ++u) {
-        const uint64_t P0 = u << S.tile_shift, P1 = std::min(P0 + T, S.g.n);
-        uint64_t best = 0;
-        int64_t bz = -1;
-        for (uint64_t a = P0; a < P1;) {
-            uint32_t lv;
-            uint64_t e;
-            btree_fix_piece(S, a, P1, lv, e);
-            if (e - a >= thr) {
-                const uint64_t z0 = btree_src_rank(S, a) >> S.tile_shift;
-                const uint64_t z1 = btree_src_rank(S, e - 1) >> S.tile_shift;
-                if (z1 - z0 <= 64)  // more runs than that are all shorter than thr
-                    for (uint64_t z = z0; z <= z1; ++z) {
-                        if (z == u) continue;
-                        uint64_t pa, pe;
-                        btree_fix_run(S, lv, a, e, z0, z1, z, pa, pe);
-                        if (pe - pa > best) {
-                            best = pe - pa;
-                            bz = (int64_t)z;
-                        }
+    const uint64_t P0 = u << S.tile_shift, P1 = P0 + T < S.g.n ? P0 + T : S.g.n;
+    uint64_t best = 0;
+    int64_t bz = -1;
+    for (uint64_t a = P0; a < P1;) {
+        uint32_t lv;
+        uint64_t e;
+        btree_fix_piece(S, a, P1, lv, e);
+        if (e - a >= thr) {
+            const uint64_t z0 = btree_src_rank(S, a) >> S.tile_shift;
+            const uint64_t z1 = btree_src_rank(S, e - 1) >> S.tile_shift;
+            if (z1 - z0 <= 64)  // more runs than that are all shorter than thr
+                for (uint64_t z = z0; z <= z1; ++z) {
+                    if (z == u) continue;
+                    uint64_t pa, pe;
+                    btree_fix_run(S, lv, a, e, z0, z1, z, pa, pe);
+                    if (pe - pa > best) {
+                        best = pe - pa;
+                        bz = (int64_t)z;
                     }
-            }
-            a = e;
+                }
         }
-        if (best >= thr) pred[u] = bz;
+        a = e;
+    }
+    return best >= thr ? bz : -1;
+}
+
+static void order_preds_range(const BtreeStream &S, std::vector<int64_t> &pred, uint64_t u0, uint64_t u1) {
+    for (uint64_t u = u0; u < u1; ++u) pred[u] = order_pred_of(S, u);
+}
+
+// Scratch keys of tile u under the ticket table tab: the count of the runs
+// btree_fix_tile_host visits (same two cases), by the lanes of one warp (each
+// takes every 32nd source tile of a piece, or every 32nd position of a dense
+// piece); the caller adds the lanes' parts.
+__device__ uint32_t order_tile_scratch(const BtreeStream &S, const uint2 *__restrict__ tab, uint64_t u,
+                                       uint32_t lane) {
+    const uint64_t P0 = u << S.tile_shift, P1 = P0 + S.tile_keys < S.g.n ? P0 + S.tile_keys : S.g.n;
+    const uint32_t ru = __ldg(tab + u).x;
+    uint32_t c = 0;
+    for (uint64_t a = P0; a < P1;) {
+        uint32_t lv;
+        uint64_t e;
+        btree_fix_piece(S, a, P1, lv, e);
+        const uint64_t z0 = btree_src_rank_at(S, lv, a) >> S.tile_shift;
+        const uint64_t z1 = btree_src_rank_at(S, lv, e - 1) >> S.tile_shift;
+        if (z1 - z0 < kFixDense) {
+            for (uint64_t z = z0 + lane; z <= z1; z += 32) {
+                if (z == u || __ldg(tab + z).x > ru) continue;
+                uint64_t pa, pe;
+                btree_fix_run(S, lv, a, e, z0, z1, z, pa, pe);
+                c += (uint32_t)(pe - pa);
+            }
+        } else {
+            for (uint64_t x = a + lane; x < e; x += 32) {
+                const uint64_t z = btree_src_rank_at(S, lv, x) >> S.tile_shift;
+                c += z != u && __ldg(tab + z).x < ru;
+            }
+        }
+        a = e;
+    }
+    return c;
+}
+
+__global__ void order_pred_kernel(const BtreeStream S, int32_t *__restrict__ pred) {
+    for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < S.ntiles;
+         u += (uint64_t)gridDim.x * blockDim.x)
+        pred[u] = (int32_t)order_pred_of(S, u);
+}
+
+// Scratch keys per tile under two ticket tables, a warp per tile.
+__global__ void order_scratch_kernel(const BtreeStream S, const uint2 *__restrict__ ta, const uint2 *__restrict__ tb,
+                                     uint32_t *__restrict__ ca, uint32_t *__restrict__ cb) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < S.ntiles; u += warps) {
+        const uint32_t a = __reduce_add_sync(0xFFFFFFFFu, order_tile_scratch(S, ta, u, lane));
+        const uint32_t b = __reduce_add_sync(0xFFFFFFFFu, order_tile_scratch(S, tb, u, lane));
+        if (lane == 0) {
+            ca[u] = a;
+            cb[u] = b;
+        }
     }
 }
 
 // Tickets by decreasing chain depth m (counting sort), ties in position order
-// (asc) or against it; then the tiles that receive scratch keys, each given a
-// tile of scratch.  Returns the number of scratch keys.
-static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, bool asc, OrderVectors &v) {
-    const uint64_t N = S.ntiles;
+// (asc) or against it.
+static void order_tickets(uint64_t N, const std::vector<uint8_t> &m, bool asc, OrderVectors &v) {
     std::vector<uint64_t> start(kChainCap + 1, 0);
     for (uint64_t u = 0; u < N; ++u) ++start[m[u]];
     uint64_t acc = 0;
@@ -113,19 +172,15 @@ static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, boo
         v.order[t] = (uint32_t)u;
         v.tab[u].x = (uint32_t)t;
     }
+}
+
+// Given each tile's scratch keys under v's tickets: the tiles that receive
+// scratch keys, each given a tile of scratch; the runs of whole scratch tiles
+// for the bulk-copy engine; the fix pass's segments for the rest.  Returns the
+// number of scratch keys.
+static uint64_t order_finish(BtreeStream S, const std::vector<uint32_t> &cnt, OrderVectors &v) {
+    const uint64_t N = S.ntiles;
     S.tab = v.tab.data();
-    // scratch keys per tile (each tile's count depends on the ticket table only)
-    std::vector<uint32_t> cnt(N, 0);
-    parallel_tiles(N, [&](uint64_t u0, uint64_t u1) {
-        for (uint64_t u = u0; u < u1; ++u) {
-            uint64_t c = 0;
-            btree_fix_tile_host(S, u, [&](uint64_t, uint64_t len) {
-                c += len;
-                return true;
-            });
-            cnt[u] = (uint32_t)c;
-        }
-    });
     std::vector<uint8_t> full(N, 0);
     uint64_t keys = 0, slots = 0;
     for (uint64_t u = 0; u < N; ++u) {
@@ -178,14 +233,31 @@ static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, boo
     return keys;
 }
 
-void btree_compute_order(const BtreeStream &S0, OrderVectors &v) {
-    BtreeStream S = S0;
-    S.plan = PLAN_O;
+// Tickets in one tie order, the tiles' scratch counts on the host's threads,
+// and the rest of the tables.
+static uint64_t order_by_depth(BtreeStream S, const std::vector<uint8_t> &m, bool asc, OrderVectors &v) {
     const uint64_t N = S.ntiles;
-    std::vector<int64_t> pred;
-    order_preds(S, pred);
-    // chain depths, each path walked once (state 1: on the current path)
-    std::vector<uint8_t> m(N, 0), state(N, 0);
+    order_tickets(N, m, asc, v);
+    S.tab = v.tab.data();
+    std::vector<uint32_t> cnt(N, 0);
+    parallel_tiles(N, [&](uint64_t u0, uint64_t u1) {
+        for (uint64_t u = u0; u < u1; ++u) {
+            uint64_t c = 0;
+            btree_fix_tile_host(S, u, [&](uint64_t, uint64_t len) {
+                c += len;
+                return true;
+            });
+            cnt[u] = (uint32_t)c;
+        }
+    });
+    return order_finish(S, cnt, v);
+}
+
+// Chain depths m(u) = 1 + m(pred(u)) (0 without a pred, kChainCap on a
+// cycle), each path walked once (state 1: on the current path).
+static void order_chains(uint64_t N, const std::vector<int64_t> &pred, std::vector<uint8_t> &m) {
+    m.assign(N, 0);
+    std::vector<uint8_t> state(N, 0);
     std::vector<uint64_t> path;
     for (uint64_t u = 0; u < N; ++u) {
         if (state[u] == 2) continue;
@@ -203,6 +275,16 @@ void btree_compute_order(const BtreeStream &S0, OrderVectors &v) {
             cur = std::min<uint32_t>(kChainCap, cur + 1);
         }
     }
+}
+
+void btree_compute_order(const BtreeStream &S0, OrderVectors &v) {
+    BtreeStream S = S0;
+    S.plan = PLAN_O;
+    const uint64_t N = S.ntiles;
+    std::vector<int64_t> pred;
+    order_preds(S, pred);
+    std::vector<uint8_t> m;
+    order_chains(N, pred, m);
     // both tie orders (right to left, left to right), side by side; keep the
     // one with fewer scratch keys (right to left on a tie)
     OrderVectors w0, w1;
@@ -211,6 +293,60 @@ void btree_compute_order(const BtreeStream &S0, OrderVectors &v) {
     c0 = order_by_depth(S, m, false, w0);
     t1.join();
     std::swap(v, c1 < c0 ? w1 : w0);
+}
+
+// The same tables with the two per-tile passes (pred, and the scratch counts
+// under both tie orders) run as kernels on st; the chain walk, the tickets
+// and the rest stay on the host.  False (nothing cached) on any CUDA failure.
+bool btree_compute_order_device(const BtreeStream &S0, cudaStream_t st, OrderVectors &v) {
+    BtreeStream S = S0;
+    S.plan = PLAN_O;
+    const uint64_t N = S.ntiles;
+    const size_t b_pred = (N * 4 + 255) / 256 * 256, b_tab = (N * 8 + 255) / 256 * 256, b_cnt = b_pred;
+    char *buf = static_cast<char *>(workspace_acquire(b_pred + 2 * b_tab + 2 * b_cnt));
+    if (!buf) return false;
+    int32_t *d_pred = reinterpret_cast<int32_t *>(buf);
+    uint2 *d_ta = reinterpret_cast<uint2 *>(buf + b_pred), *d_tb = reinterpret_cast<uint2 *>(buf + b_pred + b_tab);
+    uint32_t *d_ca = reinterpret_cast<uint32_t *>(buf + b_pred + 2 * b_tab);
+    uint32_t *d_cb = reinterpret_cast<uint32_t *>(buf + b_pred + 2 * b_tab + b_cnt);
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((N + 127) / 128, 1u << 20));
+    bool ok = true;
+    std::vector<int32_t> p32(N);
+    order_pred_kernel<<<grid, 128, 0, st>>>(S, d_pred);
+    ok = cudaMemcpyAsync(p32.data(), d_pred, N * 4, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+         cudaStreamSynchronize(st) == cudaSuccess;
+    OrderVectors w0, w1;
+    std::vector<uint32_t> n0(N), n1(N);
+    if (ok) {
+        std::vector<int64_t> pred(p32.begin(), p32.end());
+        std::vector<uint8_t> m;
+        order_chains(N, pred, m);
+        order_tickets(N, m, false, w0);
+        order_tickets(N, m, true, w1);
+        ok = cudaMemcpyAsync(d_ta, w0.tab.data(), N * 8, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+             cudaMemcpyAsync(d_tb, w1.tab.data(), N * 8, cudaMemcpyHostToDevice, st) == cudaSuccess;
+        const unsigned wgrid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((N + 7) / 8, 1u << 20));
+        if (ok) order_scratch_kernel<<<wgrid, 256, 0, st>>>(S, d_ta, d_tb, d_ca, d_cb);
+        ok = ok && cudaMemcpyAsync(n0.data(), d_ca, N * 4, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+             cudaMemcpyAsync(n1.data(), d_cb, N * 4, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+             cudaStreamSynchronize(st) == cudaSuccess && cudaGetLastError() == cudaSuccess;
+    }
+    if (!ok) {
+        cudaGetLastError();
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+    }
+    workspace_release(buf);
+    if (!ok) return false;
+    uint64_t c0 = 0, c1 = 0;
+    for (uint64_t u = 0; u < N; ++u) {
+        c0 += n0[u];
+        c1 += n1[u];
+    }
+    const bool ltr = c1 < c0;  // right to left on a tie
+    order_finish(S, ltr ? n1 : n0, ltr ? w1 : w0);
+    std::swap(v, ltr ? w1 : w0);
+    return true;
 }
 
 namespace {
@@ -235,6 +371,31 @@ OrderEntry *order_entry_locked(const BtreeStream &S) {
     return g_orders.back().get();
 }
 }  // namespace
+
+bool btree_order_prepare(const BtreeStream &S, cudaStream_t st) {
+    {
+        std::lock_guard<std::mutex> lk(g_order_mu);
+        for (auto &e : g_orders)
+            if (e->n == S.g.n && e->b == S.g.b && e->tile_keys == S.tile_keys) return true;
+        if (g_orders.size() >= kMaxOrderEntries) return false;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return false;
+    }
+    auto e = std::make_unique<OrderEntry>();
+    e->n = S.g.n;
+    e->b = S.g.b;
+    e->tile_keys = S.tile_keys;
+    if (!btree_compute_order_device(S, st, e->v)) return false;
+    std::lock_guard<std::mutex> lk(g_order_mu);
+    for (auto &x : g_orders)
+        if (x->n == S.g.n && x->b == S.g.b && x->tile_keys == S.tile_keys) return true;  // another thread's
+    if (g_orders.size() >= kMaxOrderEntries) return false;
+    g_orders.push_back(std::move(e));
+    return true;
+}
 
 bool btree_order_host(const BtreeStream &S, OrderTables &t) {
     std::lock_guard<std::mutex> lk(g_order_mu);

@@ -54,6 +54,17 @@ struct OrderVectors {
 // Computes the tables for the geometry of S (S.plan and its tables are ignored).
 void btree_compute_order(const BtreeStream &S, OrderVectors &v);
 
+// The same tables with their two per-tile passes (pred, and the scratch counts
+// under both tie orders) as kernels on st; the chain walk, the tickets and the
+// rest on the host.  False on any CUDA failure (v then undefined).
+bool btree_compute_order_device(const BtreeStream &S, cudaStream_t st, OrderVectors &v);
+
+// Computes and caches S's tables with kernels on st (their two per-tile passes)
+// when they are not cached yet; false if that cannot be done (the cache is
+// full, st is being captured, a CUDA call failed): btree_order_host then
+// computes them on the host.
+bool btree_order_prepare(const BtreeStream &S, cudaStream_t st);
+
 // Cached host tables for S's geometry; false when the cache is full.
 bool btree_order_host(const BtreeStream &S, OrderTables &t);
 

@@ -186,6 +186,10 @@ int tl_debug_permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t k
     return permute_scratch_keys(layout, n, b, key_bytes, keys);
 }
 
+int tl_debug_order_tables_match(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, void *stream) {
+    return debug_order_tables_match(layout, n, b, key_bytes, S(stream));
+}
+
 // Measurement hook: query kernel variants (0: the default).
 void tl_debug_set_query_variant(int v) { set_query_variant(v); }
 

@@ -107,6 +107,7 @@ bool ordered_schedule_forced();
 int stream_blocks_per_sm(int layout, uint32_t key_bytes);
 int last_permute_launches();
 int permute_scratch_keys(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, uint64_t *keys);
+int debug_order_tables_match(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, cudaStream_t st);
 int emulate_permute(int layout, uint64_t n, uint64_t b, uint64_t *A, uint64_t *violations);
 // query.cu: kernel selection for measurements (0: the default)
 void set_query_variant(int v);

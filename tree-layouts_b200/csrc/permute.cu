@@ -280,6 +280,14 @@ bool fixed_schedule_only() { return g_schedule_mode == 1; }
 bool ordered_schedule_forced() { return g_schedule_mode == 2; }
 
 // Plan O's tables come from the library's cache unless `tables` are given.
+// Whether a B-tree / BST plan takes the ordered-tile schedule in order_mode.
+static bool order_wanted(const PermutePlan &pl, int order_mode) {
+    return pl.bs.g.h >= 1 && pl.ntiles >= 2 &&
+           (order_mode == ORDER_ALWAYS ||
+            (order_mode == ORDER_AUTO && pl.ntiles >= (pl.b == 1 ? kOrderMinTilesBst : kOrderMinTiles) &&
+             !fixed_schedule_only()));
+}
+
 static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, PermutePlan &pl,
                      int order_mode = ORDER_AUTO, const OrderTables *tables = nullptr) {
     if (key_bytes != 4 && key_bytes != 8) return TL_ERROR_INVALID_VALUE;
@@ -314,10 +322,7 @@ static int make_plan(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, Per
         pl.ntiles = (n + pl.tile_keys - 1) / pl.tile_keys;
         pl.bs.ntiles = pl.ntiles;
         btree_choose_plan(pl.bs, key_bytes);
-        if (pl.bs.g.h >= 1 && pl.ntiles >= 2 &&
-            (order_mode == ORDER_ALWAYS ||
-             (order_mode == ORDER_AUTO && pl.ntiles >= (b == 1 ? kOrderMinTilesBst : kOrderMinTiles) &&
-              !fixed_schedule_only()))) {
+        if (order_wanted(pl, order_mode)) {
             if (tables) pl.ot = *tables;
             if (tables || btree_order_host(pl.bs, pl.ot)) {
                 btree_set_ordered(pl.bs, pl.ot.tab, pl.ot.order, pl.ot.scratch_tiles);
@@ -550,6 +555,14 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
     if (reinterpret_cast<uintptr_t>(dev_A) % (key_bytes ? key_bytes : 1)) return TL_ERROR_INVALID_VALUE;
     if (dev_ws && reinterpret_cast<uintptr_t>(dev_ws) % 256) return TL_ERROR_INVALID_VALUE;
     PermutePlan pl;
+    if (allow_ordered && n > 1 && !is_veb_layout(layout)) {
+        // a geometry not seen before: its ordered-tile tables with kernels on
+        // st (make_plan below finds them cached; if this cannot be done it
+        // computes them on the host)
+        PermutePlan fx;
+        if (make_plan(layout, n, b, key_bytes, fx, ORDER_NEVER) == TL_SUCCESS && order_wanted(fx, ORDER_AUTO))
+            btree_order_prepare(fx.bs, st);
+    }
     int rc = make_plan(layout, n, b, key_bytes, pl, allow_ordered ? ORDER_AUTO : ORDER_NEVER);
     if (rc) return rc;
     if (n <= 1) {
@@ -609,6 +622,37 @@ int permute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_bytes,
     if (rc == TL_SUCCESS && ms) *ms = timer.elapsed();
     if (rc == TL_SUCCESS && phase_ms) timer.elapsed_split(&phase_ms[0], &phase_ms[1]);
     return rc;
+}
+
+// Test hook: the ordered-tile tables of a geometry computed on the host and
+// with the per-tile kernels on st, uncached, compared entry by entry.  1 equal,
+// 0 different, < 0 a status (the geometry takes no ordered tables, or the
+// kernels could not run).
+int debug_order_tables_match(int layout, uint64_t n, uint64_t b, uint32_t key_bytes, cudaStream_t st) {
+    PermutePlan fx;
+    int rc = make_plan(layout, n, b, key_bytes, fx, ORDER_NEVER);
+    if (rc) return -rc;
+    if (is_veb_layout(layout) || !order_wanted(fx, ORDER_ALWAYS)) return -TL_ERROR_UNSUPPORTED;
+    OrderVectors h, g;
+    btree_compute_order(fx.bs, h);
+    if (!btree_compute_order_device(fx.bs, st, g)) return -TL_ERROR_CUDA;
+    auto eq2 = [](const std::vector<uint2> &x, const std::vector<uint2> &y) {
+        if (x.size() != y.size()) return false;
+        for (size_t i = 0; i < x.size(); ++i)
+            if (x[i].x != y[i].x || x[i].y != y[i].y) return false;
+        return true;
+    };
+    auto eq4 = [](const std::vector<uint4> &x, const std::vector<uint4> &y) {
+        if (x.size() != y.size()) return false;
+        for (size_t i = 0; i < x.size(); ++i)
+            if (x[i].x != y[i].x || x[i].y != y[i].y || x[i].z != y[i].z || x[i].w != y[i].w) return false;
+        return true;
+    };
+    bool same = eq2(h.tab, g.tab) && h.order == g.order && eq4(h.ranges, g.ranges) &&
+                h.scratch_tiles == g.scratch_tiles && h.segs.size() == g.segs.size();
+    for (size_t i = 0; same && i < h.segs.size(); ++i)
+        same = h.segs[i].dst_len == g.segs[i].dst_len && h.segs[i].src == g.segs[i].src;
+    return same ? 1 : 0;
 }
 
 // Host replay of the stream + scatter passes on a host array, one tile at a time
