@@ -524,27 +524,51 @@ LAYOUT_WORKLOADS = ["btree-b16-n2^30-u64", "bst-n2^30-1-u64", "mveb-n2^30-1-u32"
 def layouts_section(args, L, dev, stream, local, peak, peak_kind):
     """The permutation of 2^30-class arrays into every layout, each timed like
     the headline (device time, W warm-up and K timed steps, clocks sampled) and
-    checked bit for bit against the CPU checker after the timed steps."""
+    checked bit for bit against the CPU checker after the timed steps; then
+    2^27 plain queries on the layout (median of 3 after 2 warm-up batches),
+    a 2^20 sample of the answers checked against the CPU checker."""
     import torch
 
     from tree_layouts import data
+    import tree_layouts as T
     P = parity_module()
     out = {}
     for name in LAYOUT_WORKLOADS:
-        layout, b, n, kb, gap_hi, kseed, _, _ = WORKLOADS[name]
+        layout, b, n, kb, gap_hi, kseed, q, qseed = WORKLOADS[name]
         pristine = data.sorted_keys_torch(n, 1, gap_hi, kseed, kb, dev)
         A = torch.empty_like(pristine)
         t_stream, t_pass2, clk = time_permutation(L, layout, b, n, kb, pristine, A, stream, args.warmup,
                                                   args.steps, 1, local)
         st = permute_stats(L, layout, b, n, kb, t_stream, t_pass2, peak, peak_kind)
-        rep, _ = P.check_layout(layout, b or 16, pristine, A)
+        keep = args.layout_queries and q > 0
+        rep, host = P.check_layout(layout, b or 16, pristine, A, keep_host=keep)
         out[name] = {"layout": layout, "n": n, "key_bytes": kb,
                      "keys": f"prefix sums of uniform gaps in [1,{gap_hi}], seed {kseed}",
                      "whole_GBps": st["whole_GBps"], "whole_permute_frac": st["whole_permute_frac"],
                      "ms": st["whole_ms"], "stream_frac": st["frac"], "stream_ms": st["stream_ms"],
                      "pass2_ms": st["pass2_ms"], "schedule": st["schedule"], "kernel": st["kernel"],
                      "stalled_waits": st["stalled_waits"], "steps": args.steps, "clocks": clk, "parity": rep}
-        del pristine, A
+        if keep:
+            # the plain queries of the layout (device time; BST and vEB batches
+            # this large are searched grouped by value, the grouping included)
+            Q = data.queries_torch(pristine, q, 0.5, qseed)
+            ans = torch.empty(q, dtype=torch.int64, device=dev)
+            tabs = T.VebTablesDevice(n, dev, standard=layout == "veb") if layout in ("mveb", "veb") else None
+            for _ in range(2):
+                T.query(layout, A, Q, ans, b or 16, tables=tabs)
+            qms = statistics.median([T.query(layout, A, Q, ans, b or 16, tables=tabs, timed=True)
+                                     for _ in range(3)])
+            qbytes, l2lv, nlv = query_bytes_model(layout, n, b or 16, kb)
+            qps = q / (qms * 1e-3)
+            grouped = layout != "btree" and n * kb >= (256 << 20 if layout == "bst" else 1 << 30)
+            out[name]["queries"] = {
+                "q": q, "ms": round(qms, 3), "queries_per_s": round(qps, 1),
+                "frac_of_byte_model": round(qps * qbytes / (peak * 1e9), 4), "bytes_per_query": qbytes,
+                "kernel": query_kernel_name(layout, b or 16, kb) + (", batch grouped by value" if grouped else ""),
+                "hits": int((ans != n).sum().item()),
+                "parity": P.check_answers(layout, b or 16, host, Q, ans, 1 << 20, qseed)}
+            del Q, ans, tabs
+        del pristine, A, host
         torch.cuda.empty_cache()
     return out
 
@@ -801,6 +825,8 @@ def main():
     ap.add_argument("--batch-hi", type=int, default=22, help="batched arrays: log2 of the largest size (profiling runs)")
     ap.add_argument("--batch-tune", type=int, default=1, help="batched: run the autotuner first (0: default tuning)")
     ap.add_argument("--parity", type=int, default=1, help="bit-exact check against the CPU checker (untimed)")
+    ap.add_argument("--layout-queries", type=int, default=1,
+                    help="time 2^27 plain queries on each layout of the layouts section")
     ap.add_argument("--layouts", type=int, default=1,
                     help="every layout at 2^30-class sizes, timed and checked (default workload only)")
     ap.add_argument("--query-variant", type=int, default=0,

@@ -719,6 +719,7 @@ struct AsyncBuffer {
 
 static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStream_t st) {
     AsyncBuffer tk_buf(st), tot_buf(st);
+    keep_pool_memory();
     TL_CUDA_TRY(cudaMallocAsync(&tk_buf.p, sizeof(P.tile_keys), st));
     TL_CUDA_TRY(cudaMallocAsync(&tot_buf.p, sizeof(BatchTotals), st));
     uint32_t *d_tk = static_cast<uint32_t *>(tk_buf.p);
@@ -747,6 +748,7 @@ static int build_plan(tl_batch_plan_impl &P, const int64_t *dev_offsets, cudaStr
     P.owner = P.tile = nullptr;
     const uint64_t nowner = P.tot.tiles + P.tot.chunks;
     if (nowner) {
+        keep_pool_memory();
         TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&P.owner), nowner * sizeof(uint32_t), st));
         TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&P.tile),
                                     std::max<uint64_t>(P.tot.tiles, 1) * sizeof(uint32_t), st));
@@ -908,6 +910,7 @@ static int launch_batch_query(const tl_batch_plan_impl &P, const K *keys, const 
     auto kern = batch_query_kernel<K>;
     TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     uint32_t *d_pin = nullptr;
+    keep_pool_memory();
     TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_pin), sizeof(P.pin_levels), st));
     TL_CUDA_TRY(cudaMemcpyAsync(d_pin, P.pin_levels, sizeof(P.pin_levels), cudaMemcpyHostToDevice, st));
     int per_sm = 0;

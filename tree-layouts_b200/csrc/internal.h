@@ -86,6 +86,9 @@ int read_error_word(const unsigned int *dev_word, unsigned int *out, cudaStream_
 // work on its stream has finished.
 void *workspace_acquire(size_t bytes);
 void workspace_release(void *p);
+// Raises the current device's default pool release threshold (once per device)
+// so that stream-ordered allocations are reused across calls.
+void keep_pool_memory();
 int sync_and_check(cudaStream_t st);
 struct Ctrl;
 // Keeps the wait statistics of a permutation's control block (tl_debug_wait_stats).

@@ -997,6 +997,7 @@ int rank_model_gradient(const tl_rank_model *m, const float *dx, const float *dy
     const uint32_t blocks = (count + kTrainThreads - 1) / kTrainThreads;
     float *buf = nullptr;
     const size_t bytes = ((size_t)blocks * kParams + blocks + 2 * (kParams + 1)) * sizeof(float);
+    keep_pool_memory();
     TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&buf), bytes, st));
     float *partial = buf, *lp = buf + (size_t)blocks * kParams, *g = lp + blocks, *w = g + kParams + 1;
     float flat[kParams + 1] = {0};
@@ -1046,6 +1047,7 @@ int rank_model_train(const uint64_t *keys, uint64_t n, const tl_rank_train_confi
     float *buf = nullptr;
     const size_t nfl = (size_t)blocks * kParams + blocks + 4 * (kParams + 1);
     unsigned long long *ext = nullptr;
+    keep_pool_memory();
     TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&buf), nfl * sizeof(float), st));
     TL_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&ext), 4ull * L * sizeof(unsigned long long), st));
     float *partial = buf, *lp = partial + (size_t)blocks * kParams, *grad = lp + blocks;

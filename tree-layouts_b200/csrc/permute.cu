@@ -435,22 +435,6 @@ static int launch_permute_k(const PermutePlan &pl, K *A, char *ws, cudaStream_t 
     return TL_SUCCESS;
 }
 
-// The library's own workspaces come from the device's stream-ordered pool; keep
-// freed blocks in the pool (instead of returning them to the driver at every
-// synchronisation) so repeated calls reuse them without re-mapping memory.
-static void keep_pool_memory() {
-    static std::once_flag once[64];
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
-    std::call_once(once[dev], [dev] {
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-            uint64_t keep = UINT64_MAX;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        }
-    });
-}
-
 int btree_plan_of(uint64_t n, uint64_t b) {
     PermutePlan pl;
     if (make_plan(TL_LAYOUT_BTREE, n, b, 8, pl, ORDER_NEVER)) return -1;

@@ -690,6 +690,7 @@ static int partition_queries(const K *Q, uint64_t q, cudaStream_t st, QueryParti
     // and of this one | two (vals, idx) buffers
     const uint64_t b_mm = 256, b_c = al(kPartBuckets * 4ull), b_v = al(q * sizeof(K)), b_i = al(q * 4);
     char *buf = nullptr;
+    keep_pool_memory();
     if (cudaMallocAsync(reinterpret_cast<void **>(&buf), b_mm + 3 * b_c + 2 * (b_v + b_i), st) != cudaSuccess) {
         cudaGetLastError();
         return TL_ERROR_OUT_OF_MEMORY;

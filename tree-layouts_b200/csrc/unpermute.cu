@@ -240,6 +240,7 @@ int unpermute(int layout, void *dev_A, uint64_t n, uint64_t b, uint32_t key_byte
         if (ws) {
             owned = true;
         } else {  // the cache could not help: a stream-ordered allocation
+            keep_pool_memory();
             if (cudaMallocAsync(reinterpret_cast<void **>(&ws), need, st) != cudaSuccess) {
                 record_cuda_error(cudaGetLastError());
                 return TL_ERROR_OUT_OF_MEMORY;

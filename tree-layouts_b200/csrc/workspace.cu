@@ -67,6 +67,28 @@ void *workspace_acquire(size_t bytes) {
     return p;
 }
 
+// The library's stream-ordered allocations (query partitions, batched plans,
+// rank-model training, and workspaces the cache cannot provide) come from the
+// device's default pool; keep freed blocks in the pool instead of returning
+// them to the driver at every synchronisation, so repeated calls reuse them
+// without re-mapping memory (a 250 MB re-map took 27 to 79 ms on B200).
+void keep_pool_memory() {
+    static std::once_flag once[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return;
+    }
+    std::call_once(once[dev], [dev] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    });
+}
+
 void workspace_release(void *p) {
     std::lock_guard<std::mutex> lk(g_ws_mu);
     for (auto &b : g_ws)
