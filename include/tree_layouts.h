@@ -199,8 +199,8 @@ int tl_query_sorted_u64(const uint64_t *dev_sorted, uint64_t n, const uint64_t *
                         uint64_t q, uint64_t *dev_answers, void *stream, float *ms);
 /* BST and vEB queries: a batch of 2^20 queries or more over a layout of at
  * least 256 MB (BST) or 1 GB (vEB) is first grouped by value, in
- * stream-ordered temporary device memory of about q * (2 w + 8) bytes (w the
- * key width), so that queries close in value share the deep nodes they fetch;
+ * stream-ordered temporary device memory of about q * (2 w + 8) bytes plus
+ * 16 MB (w the key width), so that queries close in value share the deep nodes they fetch;
  * the answers keep the batch's order.  If that memory cannot be had, the batch
  * is searched as given.
  *

@@ -507,19 +507,24 @@ veb_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, uint32_t dmax,
 // Queries close in value walk close paths through a BST or vEB layout, whose
 // lower levels hold each subtree's keys together.  Grouping a batch by value
 // lets a node fetched once from HBM serve the rest of its group from L2 or L1.
-// The batch is split into 65536 buckets of its value range [min q, max q]
-// (digit = (q - min q) >> shift, shift fitting the range to 16 bits) by four
+// The batch is split into 2^20 buckets of its value range [min q, max q]
+// (bucket = (q - min q) >> shift, shift fitting the range to 20 bits) by five
 // passes over 4 bits each, most significant first.  A pass gives every block
 // tiles of kPartTile entries; within each segment of the previous pass that a
 // tile touches it ranks the entries into 16 bins in shared memory, reserves
 // one global range per (segment, bin) with a single atomic, and writes each
-// bin's entries out as one contiguous run.  Order within a bucket is not kept
-// (the search does not need it).  The search kernels write each answer
-// through the carried index, so the answers keep the batch's order.
-constexpr uint32_t kPartBits = 16, kPartBuckets = 1u << kPartBits;
+// bin's entries out as one contiguous run.  The same pass counts the entries
+// of every (segment, bin) by the next digit, so only the first pass needs a
+// counting sweep of its own.  Order within a bucket is not kept (the search
+// does not need it).  The search kernels write each answer through the
+// carried index, so the answers keep the batch's order.
+constexpr uint32_t kPartBits = 20, kPartBuckets = 1u << kPartBits;
 constexpr uint32_t kPartDigit = 4, kPartBins = 1u << kPartDigit, kPartPasses = kPartBits / kPartDigit;
 constexpr int kPartThreads = 256;
-// entries per tile: the staging area of values and indices in under 48 KB
+constexpr uint32_t kPartScanChunk = 4096;  // counts scanned by one block of 1024 threads
+static_assert(kPartBins * kPartBins == kPartThreads, "one next-digit counter per thread");
+static_assert(kPartBuckets / kPartScanChunk <= 1024, "chunk totals fit one block");
+// entries per tile: the staging area of values, indices and bins in under 48 KB
 template <typename K>
 constexpr uint32_t part_tile() {
     return sizeof(K) == 8 ? 3584 : 4096;
@@ -554,53 +559,104 @@ __global__ void qpart_minmax_kernel(const K *__restrict__ Q, uint64_t q, unsigne
     }
 }
 
-__device__ __forceinline__ uint32_t qpart_digit(uint64_t v, const unsigned long long *mm) {
+// The bucket of value v is the kPartBits bits of (v - min q) below the top of
+// the range [min q, max q]: (v - min q) >> qpart_bucket_shift(mm)
+__device__ __forceinline__ uint32_t qpart_bucket_shift(const unsigned long long *mm) {
     const uint32_t bits = bit_length((uint64_t)(mm[1] - mm[0]));
-    return (uint32_t)(((v - mm[0]) >> (bits > kPartBits ? bits - kPartBits : 0)) & (kPartBuckets - 1));
+    return bits > kPartBits ? bits - kPartBits : 0;
 }
 
-// One pass (pass p takes digit bits [kPartBits - 4(p+1), kPartBits - 4p)) over
-// entries [0, q) of (vals, idx) (idx == nullptr: the entry's own index).
+// The first segment s in [lo, nseg) whose end seg_end[s] is above a, found by
+// one warp: each round probes 32 ends spread over the open range.  Needs
+// seg_end non-decreasing, seg_end[s] <= a for s < lo and seg_end[nseg - 1] > a.
+// consecutive: probe lo .. lo + 31 first (a portion that ended at a segment's
+// end is usually followed by the next segment).
+__device__ __forceinline__ uint32_t qpart_find_segment(const uint32_t *__restrict__ seg_end, uint32_t lo,
+                                                       uint32_t nseg, uint64_t a, bool consecutive) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t hi = nseg;
+    uint32_t step = consecutive ? 1 : (hi - lo + 31) / 32;
+    for (;;) {
+        const uint32_t at = min(lo + (lane + 1) * step - 1, hi - 1);
+        const uint32_t hit = __ballot_sync(0xFFFFFFFFu, seg_end[at] > a);
+        if (hit == 0) {  // all 32 probes at or below a (only in a consecutive round below hi)
+            lo += 32 * step;
+            step = (hi - lo + 31) / 32;
+            continue;
+        }
+        const uint32_t f = __ffs(hit) - 1;
+        const uint32_t at_f = min(lo + (f + 1) * step - 1, hi - 1);
+        if (step == 1) return at_f;
+        lo += f * step;  // just past the probe before the first hit
+        hi = at_f + 1;
+        step = (hi - lo + 31) / 32;
+    }
+}
+
+// One pass (pass p takes bucket bits [kPartBits - 4(p+1), kPartBits - 4p))
+// over entries [0, q) of (vals, idx) (idx == nullptr: the entry's own index).
 // seg_end[0 .. nseg) are the exclusive ends of the previous pass's segments
 // (nseg = 16^p; pass 0: one segment).  mode 0 adds the tiles' bin counts to
 // count[seg * 16 + bin]; mode 1 scatters through cursor[] (count[] scanned)
-// into (ovals, oidx).
+// into (ovals, oidx) and, with next != nullptr, adds the counts of the next
+// digit to next[(seg * 16 + bin) * 16 + next digit].
 template <typename K>
 __global__ void __launch_bounds__(kPartThreads)
 qpart_pass_kernel(int mode, uint32_t pass, const K *__restrict__ vals, const uint32_t *__restrict__ idx, uint64_t q,
                   const unsigned long long *__restrict__ mm, const uint32_t *__restrict__ seg_end, uint32_t nseg,
-                  uint32_t *__restrict__ count, K *__restrict__ ovals, uint32_t *__restrict__ oidx) {
+                  uint32_t *__restrict__ count, K *__restrict__ ovals, uint32_t *__restrict__ oidx,
+                  uint32_t *__restrict__ next) {
     constexpr uint32_t kPartTile = part_tile<K>();
+    constexpr int kItems = kPartTile / kPartThreads;
     __shared__ K sv[kPartTile];
     __shared__ uint32_t si[kPartTile];
+    __shared__ uint8_t sb[kPartTile];  // the bin of each staged entry
     __shared__ uint32_t cnt[kPartBins], off[kPartBins], run[kPartBins], base[kPartBins];
+    __shared__ uint32_t nxt[kPartBins * kPartBins];
     __shared__ uint32_t s_seg[2];
-    const uint32_t shift = kPartBits - kPartDigit * (pass + 1);
+    const uint64_t qmin = mm[0];
+    const uint32_t shift = qpart_bucket_shift(mm) + kPartBits - kPartDigit * (pass + 1);  // this digit
+    const bool count_next = mode == 1 && next != nullptr && pass + 1 < kPartPasses;
     for (uint64_t t0 = (uint64_t)blockIdx.x * kPartTile; t0 < q; t0 += (uint64_t)gridDim.x * kPartTile) {
         const uint64_t t1 = min(q, t0 + kPartTile);
         uint64_t a = t0;
+        uint32_t seg = 0;
         while (a < t1) {  // one segment of the previous pass at a time
             __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t lo = 0, hi = nseg - 1;  // the segment holding entry a: first end above a
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi) / 2;
-                    if (seg_end[mid] > a) hi = mid; else lo = mid + 1;
+            if (threadIdx.x < 32) {  // the segment holding entry a
+                const uint32_t s =
+                    nseg > 1 ? qpart_find_segment(seg_end, a == t0 ? 0 : seg + 1, nseg, a, a != t0) : 0;
+                if (threadIdx.x == 0) {
+                    s_seg[0] = s;
+                    s_seg[1] = nseg > 1 ? seg_end[s] : (uint32_t)q;  // pass 0: one segment [0, q)
                 }
-                s_seg[0] = lo;
-                s_seg[1] = nseg > 1 ? seg_end[lo] : (uint32_t)q;  // pass 0: one segment [0, q)
             }
             if (threadIdx.x < kPartBins) {
                 cnt[threadIdx.x] = 0;
                 run[threadIdx.x] = 0;
             }
+            nxt[threadIdx.x] = 0;
             __syncthreads();
-            const uint32_t seg = s_seg[0];
+            seg = s_seg[0];
             uint64_t b = min(t1, (uint64_t)s_seg[1]);
             if (b <= a) b = t1;  // cannot happen (the last end is q); both modes take the same steps
             const uint32_t len = (uint32_t)(b - a);
-            for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
-                atomicAdd(&cnt[(qpart_digit((uint64_t)vals[a + j], mm) >> shift) & (kPartBins - 1)], 1u);
+            // this thread's entries j = threadIdx.x + i * kPartThreads of the
+            // portion, values and indices loaded together (their latencies
+            // overlap) and kept in registers
+            K v[kItems];
+            uint32_t id[kItems];
+#pragma unroll
+            for (int i = 0; i < kItems; ++i) {
+                const uint32_t j = threadIdx.x + i * kPartThreads;
+                v[i] = j < len ? vals[a + j] : K(0);
+                id[i] = mode == 1 && idx && j < len ? idx[a + j] : (uint32_t)(a + j);
+            }
+#pragma unroll
+            for (int i = 0; i < kItems; ++i) {
+                const uint32_t j = threadIdx.x + i * kPartThreads;
+                if (j < len) atomicAdd(&cnt[(((uint64_t)v[i] - qmin) >> shift) & (kPartBins - 1)], 1u);
+            }
             __syncthreads();
             if (mode == 0) {
                 if (threadIdx.x < kPartBins && cnt[threadIdx.x])
@@ -616,56 +672,96 @@ qpart_pass_kernel(int mode, uint32_t pass, const K *__restrict__ vals, const uin
                 if (threadIdx.x < kPartBins && cnt[threadIdx.x])
                     base[threadIdx.x] = atomicAdd(&count[seg * kPartBins + threadIdx.x], cnt[threadIdx.x]);
                 __syncthreads();
-                for (uint32_t j = threadIdx.x; j < len; j += blockDim.x) {  // rank into the staging area
-                    const K v = vals[a + j];
-                    const uint32_t bin = (qpart_digit((uint64_t)v, mm) >> shift) & (kPartBins - 1);
-                    const uint32_t r = off[bin] + atomicAdd(&run[bin], 1u);
-                    sv[r] = v;
-                    si[r] = idx ? idx[a + j] : (uint32_t)(a + j);
+#pragma unroll
+                for (int i = 0; i < kItems; ++i) {  // rank into the staging area
+                    const uint32_t j = threadIdx.x + i * kPartThreads;
+                    if (j < len) {
+                        const uint64_t rel = (uint64_t)v[i] - qmin;
+                        const uint32_t bin = (uint32_t)(rel >> shift) & (kPartBins - 1);
+                        const uint32_t r = off[bin] + atomicAdd(&run[bin], 1u);
+                        sv[r] = v[i];
+                        si[r] = id[i];
+                        sb[r] = (uint8_t)bin;
+                        if (count_next)
+                            atomicAdd(&nxt[bin * kPartBins +
+                                           ((uint32_t)(rel >> (shift - kPartDigit)) & (kPartBins - 1))],
+                                      1u);
+                    }
                 }
+                if (threadIdx.x < kPartBins) base[threadIdx.x] -= off[threadIdx.x];  // bin's entry j goes to base + j
                 __syncthreads();
                 for (uint32_t j = threadIdx.x; j < len; j += blockDim.x) {  // each bin as one run
-                    // bins are ordered: the last bin starting at or below j,
-                    // stepping back over empty bins (they share a start)
-                    uint32_t bin = 0;
-#pragma unroll
-                    for (uint32_t k = 1; k < kPartBins; ++k)
-                        if (off[k] <= j) bin = k;
-                    while (cnt[bin] == 0 || off[bin] + cnt[bin] <= j) --bin;
-                    const uint32_t p = base[bin] + (j - off[bin]);
+                    const uint32_t p = base[sb[j]] + j;
                     ovals[p] = sv[j];
                     oidx[p] = si[j];
                 }
+                // (segment, bin) of this pass is segment seg * 16 + bin of the
+                // next: its counters start at (seg * 16 + bin) * 16
+                if (count_next && nxt[threadIdx.x])
+                    atomicAdd(&next[(uint64_t)seg * kPartBins * kPartBins + threadIdx.x], nxt[threadIdx.x]);
             }
             a = b;
         }
     }
 }
 
-// Exclusive scan of `m` counts (m a multiple of 1024, at most kPartBuckets)
-// in place by one block of 1024 threads; with ends != nullptr also the
-// inclusive sums (the segment ends of the next pass).
-__global__ void __launch_bounds__(1024) qpart_scan_kernel(uint32_t *__restrict__ count, uint32_t m,
-                                                          uint32_t *__restrict__ ends) {
-    const uint32_t per = m / 1024;
-    __shared__ uint32_t part[1024];
-    uint32_t *c = count + threadIdx.x * per;
-    uint32_t sum = 0;
-    for (uint32_t k = 0; k < per; ++k) sum += c[k];
-    part[threadIdx.x] = sum;
-    __syncthreads();
-    for (uint32_t off = 1; off < 1024; off <<= 1) {  // inclusive scan of the parts
-        const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
+// Exclusive scan of count[0, m) in place, m a multiple of kPartScanChunk: block
+// c scans chunk c; ends (when given) gets the inclusive sums and total[c] the
+// chunk's sum.  With more than one chunk, qpart_scan_add_kernel then adds the
+// sums of the chunks before each one.
+__global__ void __launch_bounds__(1024) qpart_scan_kernel(uint32_t *__restrict__ count, uint32_t *__restrict__ ends,
+                                                          uint32_t *__restrict__ total) {
+    static_assert(kPartScanChunk == 4 * 1024, "four counts a thread");
+    __shared__ uint32_t wsum[32];
+    const uint64_t at = (uint64_t)blockIdx.x * kPartScanChunk + threadIdx.x * 4;
+    const uint4 c = *reinterpret_cast<const uint4 *>(count + at);
+    const uint32_t sum = c.x + c.y + c.z + c.w;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = sum;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= (uint32_t)o) inc += t;
     }
-    uint32_t run = part[threadIdx.x] - sum;
-    for (uint32_t k = 0; k < per; ++k) {
-        const uint32_t v = c[k];
-        c[k] = run;
-        run += v;
-        if (ends) ends[threadIdx.x * per + k] = run;
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= (uint32_t)o) w += t;
+        }
+        wsum[lane] = w;  // inclusive over warps
+        if (lane == 31 && total) total[blockIdx.x] = w;
+    }
+    __syncthreads();
+    const uint32_t r0 = (warp ? wsum[warp - 1] : 0) + inc - sum;
+    const uint4 ex = make_uint4(r0, r0 + c.x, r0 + c.x + c.y, r0 + c.x + c.y + c.z);
+    *reinterpret_cast<uint4 *>(count + at) = ex;
+    if (ends) *reinterpret_cast<uint4 *>(ends + at) = make_uint4(ex.y, ex.z, ex.w, ex.w + c.w);
+}
+
+// Block c of the grid adds the sums of chunks [0, c + 1) to chunk c + 1.
+__global__ void __launch_bounds__(1024) qpart_scan_add_kernel(uint32_t *__restrict__ count,
+                                                              uint32_t *__restrict__ ends,
+                                                              const uint32_t *__restrict__ total) {
+    __shared__ uint32_t s_off;
+    const uint32_t chunk = blockIdx.x + 1;
+    if (threadIdx.x < 32) {
+        uint32_t o = 0;
+        for (uint32_t k = threadIdx.x; k < chunk; k += 32) o += total[k];
+        o = __reduce_add_sync(0xFFFFFFFFu, o);
+        if (threadIdx.x == 0) s_off = o;
+    }
+    __syncthreads();
+    const uint32_t o = s_off;
+    const uint64_t at = (uint64_t)chunk * kPartScanChunk + threadIdx.x * 4;
+    uint4 c = *reinterpret_cast<const uint4 *>(count + at);
+    *reinterpret_cast<uint4 *>(count + at) = make_uint4(c.x + o, c.y + o, c.z + o, c.w + o);
+    if (ends) {
+        c = *reinterpret_cast<const uint4 *>(ends + at);
+        *reinterpret_cast<uint4 *>(ends + at) = make_uint4(c.x + o, c.y + o, c.z + o, c.w + o);
     }
 }
 
@@ -686,12 +782,13 @@ struct QueryPartition {
 template <typename K>
 static int partition_queries(const K *Q, uint64_t q, cudaStream_t st, QueryPartition &out) {
     auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
-    // mm | counts of a pass (up to 65536) | segment ends of the previous pass
-    // and of this one | two (vals, idx) buffers
-    const uint64_t b_mm = 256, b_c = al(kPartBuckets * 4ull), b_v = al(q * sizeof(K)), b_i = al(q * 4);
+    // mm and the scan's chunk totals | the counts of this pass and of the
+    // next (up to 2^20 each) | segment ends of the previous pass and of this
+    // one | two (vals, idx) buffers
+    const uint64_t b_mm = 256 + 4096, b_c = al(kPartBuckets * 4ull), b_v = al(q * sizeof(K)), b_i = al(q * 4);
     char *buf = nullptr;
     keep_pool_memory();
-    if (cudaMallocAsync(reinterpret_cast<void **>(&buf), b_mm + 3 * b_c + 2 * (b_v + b_i), st) != cudaSuccess) {
+    if (cudaMallocAsync(reinterpret_cast<void **>(&buf), b_mm + 4 * b_c + 2 * (b_v + b_i), st) != cudaSuccess) {
         cudaGetLastError();
         return TL_ERROR_OUT_OF_MEMORY;
     }
@@ -699,9 +796,10 @@ static int partition_queries(const K *Q, uint64_t q, cudaStream_t st, QueryParti
     out.st = st;
     char *p = buf;
     unsigned long long *mm = reinterpret_cast<unsigned long long *>(p);
+    uint32_t *total = reinterpret_cast<uint32_t *>(p + 256);
     p += b_mm;
-    uint32_t *cnt = reinterpret_cast<uint32_t *>(p);
-    p += b_c;
+    uint32_t *cnt[2] = {reinterpret_cast<uint32_t *>(p), reinterpret_cast<uint32_t *>(p + b_c)};
+    p += 2 * b_c;
     uint32_t *ends[2] = {reinterpret_cast<uint32_t *>(p), reinterpret_cast<uint32_t *>(p + b_c)};
     p += 2 * b_c;
     K *v[2] = {reinterpret_cast<K *>(p), reinterpret_cast<K *>(p + b_v + b_i)};
@@ -712,20 +810,29 @@ static int partition_queries(const K *Q, uint64_t q, cudaStream_t st, QueryParti
     qpart_minmax_kernel<K><<<g, 256, 0, st>>>(Q, q, mm);
     const unsigned gt =
         (unsigned)std::min<uint64_t>((q + part_tile<K>() - 1) / part_tile<K>(), (uint64_t)query_sm_count() * 8);
+    auto padded = [](uint32_t m) { return (m + kPartScanChunk - 1) / kPartScanChunk * kPartScanChunk; };
     const K *src_v = Q;
     const uint32_t *src_i = nullptr;
     uint32_t nseg = 1;
+    TL_CUDA_TRY(cudaMemsetAsync(cnt[0], 0, (size_t)padded(kPartBins) * 4, st));
+    qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(0, 0, src_v, src_i, q, mm, ends[1], 1, cnt[0], nullptr, nullptr,
+                                                      nullptr);
     for (uint32_t pass = 0; pass < kPartPasses; ++pass) {
         const uint32_t m = nseg * kPartBins;  // this pass's buckets
         const uint32_t *seg = ends[(pass + 1) & 1];
         uint32_t *next_ends = ends[pass & 1];
-        TL_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)std::max<uint32_t>(m, 1024) * 4, st));
-        qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(0, pass, src_v, src_i, q, mm, seg, nseg, cnt, nullptr,
-                                                          nullptr);
-        qpart_scan_kernel<<<1, 1024, 0, st>>>(cnt, std::max<uint32_t>(m, 1024), next_ends);
+        uint32_t *count = cnt[pass & 1], *next = nullptr;
+        const uint32_t chunks = padded(m) / kPartScanChunk;
+        qpart_scan_kernel<<<chunks, 1024, 0, st>>>(count, next_ends, total);
+        if (chunks > 1) qpart_scan_add_kernel<<<chunks - 1, 1024, 0, st>>>(count, next_ends, total);
+        if (pass + 1 < kPartPasses) {
+            next = cnt[(pass + 1) & 1];
+            TL_CUDA_TRY(cudaMemsetAsync(next, 0, (size_t)padded(m * kPartBins) * 4, st));
+        }
         K *dv = v[pass & 1];
         uint32_t *di = ix[pass & 1];
-        qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(1, pass, src_v, src_i, q, mm, seg, nseg, cnt, dv, di);
+        qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(1, pass, src_v, src_i, q, mm, seg, nseg, count, dv, di,
+                                                          next);
         src_v = dv;
         src_i = di;
         nseg = m;
