@@ -560,7 +560,7 @@ def layouts_section(args, L, dev, stream, local, peak, peak_kind):
                                      for _ in range(3)])
             qbytes, l2lv, nlv = query_bytes_model(layout, n, b or 16, kb)
             qps = q / (qms * 1e-3)
-            grouped = layout != "btree" and n * kb >= (256 << 20 if layout == "bst" else 1 << 30)
+            grouped = layout != "btree" and q >= 1 << 21 and n * kb >= (64 << 20 if layout == "bst" else 4 << 20)
             out[name]["queries"] = {
                 "q": q, "ms": round(qms, 3), "queries_per_s": round(qps, 1),
                 "frac_of_byte_model": round(qps * qbytes / (peak * 1e9), 4), "bytes_per_query": qbytes,

@@ -197,11 +197,11 @@ int tl_query_sorted_u32(const uint32_t *dev_sorted, uint64_t n, const uint32_t *
                         uint64_t q, uint64_t *dev_answers, void *stream, float *ms);
 int tl_query_sorted_u64(const uint64_t *dev_sorted, uint64_t n, const uint64_t *dev_queries,
                         uint64_t q, uint64_t *dev_answers, void *stream, float *ms);
-/* BST and vEB queries: a batch of 2^20 queries or more over a layout of at
- * least 256 MB (BST) or 1 GB (vEB) is first grouped by value, in
+/* BST and vEB queries: a batch of 2^21 queries or more over a layout of at
+ * least 64 MB (BST) or 4 MB (vEB) is first grouped by value, in
  * stream-ordered temporary device memory of about q * (2 w + 8) bytes plus
- * 16 MB (w the key width), so that queries close in value share the deep nodes they fetch;
- * the answers keep the batch's order.  If that memory cannot be had, the batch
+ * up to 16 MB (w the key width), so that queries close in value share the
+ * deep nodes they fetch; the answers keep the batch's order.  If that memory cannot be had, the batch
  * is searched as given.
  *
  * dev_answers[i] = position of dev_queries[i] in the layout, or n.
@@ -395,8 +395,8 @@ int tl_debug_set_schedule(int mode);
  * place of a group of lanes per node, for the learned query too); 7 B-tree one
  * 32-byte load per lane of the group (b * w / 32 lanes); 19 BST and vEB
  * batches searched as given, 20 always grouped by value (by default only
- * batches of 2^20 queries or more over BST layouts of 256 MB or more and vEB
- * layouts of 1 GB or more). */
+ * batches of 2^21 queries or more over BST layouts of 64 MB or more and vEB
+ * layouts of 4 MB or more). */
 void tl_debug_set_query_variant(int v);
 /* Instances of a batched plan on the ordered-tile schedule and their keys: by
  * default those of 64 tiles or more (at the plan's tile size for their size

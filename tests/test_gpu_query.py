@@ -172,9 +172,10 @@ def test_veb_query_kernel_forms(variant, layout):
 @pytest.mark.parametrize("layout,n,kb", [("mveb", 2**24 - 1, 4), ("mveb", 20_000_003, 4), ("veb", 2**22 - 1, 8),
                                          ("bst", 2**23 - 1, 8), ("bst", 9_000_001, 4)])
 def test_partitioned_queries_match_unpartitioned(layout, n, kb):
-    """A batch searched grouped by value (a four-pass partition of the batch's
-    value range into 65536 buckets, answers written back through the carried
-    index; variant 20 forces it at any size) equals the batch searched as
+    """A batch searched grouped by value (a partition of the batch's value
+    range into up to 2^20 buckets, 4 bits a pass, answers written back through the carried
+    index, vEB descents in 256-thread blocks; variant 20 forces it at any
+    size) equals the batch searched as
     given (variant 19) for batch lengths around the partition's 4096-entry
     tiles, with duplicates and a batch of one value; every hit names its key's
     slot and every miss is a key absent from the sorted keys."""

@@ -386,6 +386,16 @@ int query_variant() { return g_query_variant; }
 // reference reads past its table there; it only ever issues hits).
 constexpr int kVebThreads = 128;
 constexpr size_t kVebMinPin = 8 * 1024;
+// A batch grouped by value: neighbouring descents share most deep nodes (L1
+// and L2 hits), so more of them in flight pays where it costs L1 hits on a
+// batch as given.  Measured on B200, 2^27 grouped queries over 2^30 - 1 u32
+// mvEB keys (grouping included): 128 threads and 48 KB a block 20.6 ms,
+// 128 / 24 KB 15.0, 128 / 32 KB 17.7, 256 / 40 KB 14.3, 256 / 48 KB 14.0,
+// 256 / 64 KB 16.0, 384 / 56 KB 13.6, 512 / 72 KB 13.5, 1024 / 136 KB
+// 14.7 ms; shapes with more threads on the batch as given 46.6 to 56.4 ms
+// against 40.0 (128 / 48 KB).
+constexpr int kVebGroupThreads = 512;
+constexpr size_t kVebGroupBudget = 72 * 1024;
 
 // QK descents per thread in lock-step: every step takes all of a thread's
 // unresolved queries one level down, so their key loads are in flight together
@@ -454,8 +464,8 @@ __device__ __forceinline__ void veb_descend_multi(const K *__restrict__ A, const
 // non-perfect table set (timeQueryvEB_nonperfect): the divisions in order, each
 // query until it is resolved.  A block takes QK * T consecutive queries at a
 // time, thread t the queries t, t + T, ...
-template <typename K, typename PosT, int QK>
-__global__ void __launch_bounds__(kVebThreads)
+template <typename K, typename PosT, int QK, int kThreads>
+__global__ void __launch_bounds__(kThreads)
 veb_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, uint32_t dmax,
                  const tl_veb_table *__restrict__ tables, const uint64_t *__restrict__ idx,
                  const uint32_t *__restrict__ table_idx, uint32_t num_tables, const K *__restrict__ Q,
@@ -507,9 +517,10 @@ veb_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, uint32_t dmax,
 // Queries close in value walk close paths through a BST or vEB layout, whose
 // lower levels hold each subtree's keys together.  Grouping a batch by value
 // lets a node fetched once from HBM serve the rest of its group from L2 or L1.
-// The batch is split into 2^20 buckets of its value range [min q, max q]
-// (bucket = (q - min q) >> shift, shift fitting the range to 20 bits) by five
-// passes over 4 bits each, most significant first.  A pass gives every block
+// The batch is split into 2^bits buckets of its value range [min q, max q]
+// (bucket = (q - min q) >> shift, shift fitting the range to `bits` bits) by
+// bits / 4 passes over 4 bits each, most significant first; `bits` grows with
+// the batch (part_bits) up to 20.  A pass gives every block
 // tiles of kPartTile entries; within each segment of the previous pass that a
 // tile touches it ranks the entries into 16 bins in shared memory, reserves
 // one global range per (segment, bin) with a single atomic, and writes each
@@ -518,8 +529,13 @@ veb_query_kernel(const K *__restrict__ A, uint64_t n, uint64_t P, uint32_t dmax,
 // counting sweep of its own.  Order within a bucket is not kept (the search
 // does not need it).  The search kernels write each answer through the
 // carried index, so the answers keep the batch's order.
-constexpr uint32_t kPartBits = 20, kPartBuckets = 1u << kPartBits;
-constexpr uint32_t kPartDigit = 4, kPartBins = 1u << kPartDigit, kPartPasses = kPartBits / kPartDigit;
+constexpr uint32_t kPartMaxBits = 20, kPartBuckets = 1u << kPartMaxBits;
+constexpr uint32_t kPartDigit = 4, kPartBins = 1u << kPartDigit;
+// Entries a segment of the last pass holds on average, at least: a tile that
+// meets many small segments takes one portion at a time (measured on B200,
+// 2^20 queries into 2^20 buckets: the last pass 0.61 ms, the whole search
+// 0.06 ms; 2048 measured as fast as 1024 or faster from 2^20 to 2^27 queries)
+constexpr uint64_t kPartMinSegment = 2048;
 constexpr int kPartThreads = 256;
 constexpr uint32_t kPartScanChunk = 4096;  // counts scanned by one block of 1024 threads
 static_assert(kPartBins * kPartBins == kPartThreads, "one next-digit counter per thread");
@@ -559,11 +575,11 @@ __global__ void qpart_minmax_kernel(const K *__restrict__ Q, uint64_t q, unsigne
     }
 }
 
-// The bucket of value v is the kPartBits bits of (v - min q) below the top of
-// the range [min q, max q]: (v - min q) >> qpart_bucket_shift(mm)
-__device__ __forceinline__ uint32_t qpart_bucket_shift(const unsigned long long *mm) {
-    const uint32_t bits = bit_length((uint64_t)(mm[1] - mm[0]));
-    return bits > kPartBits ? bits - kPartBits : 0;
+// The bucket of value v is the `bits` bits of (v - min q) below the top of
+// the range [min q, max q]: (v - min q) >> qpart_bucket_shift(mm, bits)
+__device__ __forceinline__ uint32_t qpart_bucket_shift(const unsigned long long *mm, uint32_t bits) {
+    const uint32_t span = bit_length((uint64_t)(mm[1] - mm[0]));
+    return span > bits ? span - bits : 0;
 }
 
 // The first segment s in [lo, nseg) whose end seg_end[s] is above a, found by
@@ -593,7 +609,7 @@ __device__ __forceinline__ uint32_t qpart_find_segment(const uint32_t *__restric
     }
 }
 
-// One pass (pass p takes bucket bits [kPartBits - 4(p+1), kPartBits - 4p))
+// One pass (pass p takes bucket bits [bits - 4(p+1), bits - 4p))
 // over entries [0, q) of (vals, idx) (idx == nullptr: the entry's own index).
 // seg_end[0 .. nseg) are the exclusive ends of the previous pass's segments
 // (nseg = 16^p; pass 0: one segment).  mode 0 adds the tiles' bin counts to
@@ -602,7 +618,7 @@ __device__ __forceinline__ uint32_t qpart_find_segment(const uint32_t *__restric
 // digit to next[(seg * 16 + bin) * 16 + next digit].
 template <typename K>
 __global__ void __launch_bounds__(kPartThreads)
-qpart_pass_kernel(int mode, uint32_t pass, const K *__restrict__ vals, const uint32_t *__restrict__ idx, uint64_t q,
+qpart_pass_kernel(int mode, uint32_t bits, uint32_t pass, const K *__restrict__ vals, const uint32_t *__restrict__ idx, uint64_t q,
                   const unsigned long long *__restrict__ mm, const uint32_t *__restrict__ seg_end, uint32_t nseg,
                   uint32_t *__restrict__ count, K *__restrict__ ovals, uint32_t *__restrict__ oidx,
                   uint32_t *__restrict__ next) {
@@ -615,8 +631,8 @@ qpart_pass_kernel(int mode, uint32_t pass, const K *__restrict__ vals, const uin
     __shared__ uint32_t nxt[kPartBins * kPartBins];
     __shared__ uint32_t s_seg[2];
     const uint64_t qmin = mm[0];
-    const uint32_t shift = qpart_bucket_shift(mm) + kPartBits - kPartDigit * (pass + 1);  // this digit
-    const bool count_next = mode == 1 && next != nullptr && pass + 1 < kPartPasses;
+    const uint32_t shift = qpart_bucket_shift(mm, bits) + bits - kPartDigit * (pass + 1);  // this digit
+    const bool count_next = mode == 1 && next != nullptr && pass + 1 < bits / kPartDigit;
     for (uint64_t t0 = (uint64_t)blockIdx.x * kPartTile; t0 < q; t0 += (uint64_t)gridDim.x * kPartTile) {
         const uint64_t t1 = min(q, t0 + kPartTile);
         uint64_t a = t0;
@@ -779,13 +795,25 @@ struct QueryPartition {
     }
 };
 
+// Bucket bits for a batch of q queries: the most (a multiple of 4, at most
+// kPartMaxBits) whose last pass still has kPartMinSegment entries a segment
+// on average, and at least 4.
+static uint32_t part_bits(uint64_t q) {
+    uint32_t bits = kPartDigit;
+    while (bits + kPartDigit <= kPartMaxBits && (q >> bits) >= kPartMinSegment) bits += kPartDigit;
+    return bits;
+}
+
 template <typename K>
 static int partition_queries(const K *Q, uint64_t q, cudaStream_t st, QueryPartition &out) {
     auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
+    auto padded = [](uint32_t m) { return (m + kPartScanChunk - 1) / kPartScanChunk * kPartScanChunk; };
+    const uint32_t bits = part_bits(q), passes = bits / kPartDigit;
     // mm and the scan's chunk totals | the counts of this pass and of the
-    // next (up to 2^20 each) | segment ends of the previous pass and of this
-    // one | two (vals, idx) buffers
-    const uint64_t b_mm = 256 + 4096, b_c = al(kPartBuckets * 4ull), b_v = al(q * sizeof(K)), b_i = al(q * 4);
+    // next (up to 2^bits each) | segment ends of the previous pass and of
+    // this one | two (vals, idx) buffers
+    const uint64_t b_mm = 256 + 4096, b_c = al(padded(1u << bits) * 4ull), b_v = al(q * sizeof(K)),
+                   b_i = al(q * 4);
     char *buf = nullptr;
     keep_pool_memory();
     if (cudaMallocAsync(reinterpret_cast<void **>(&buf), b_mm + 4 * b_c + 2 * (b_v + b_i), st) != cudaSuccess) {
@@ -810,14 +838,13 @@ static int partition_queries(const K *Q, uint64_t q, cudaStream_t st, QueryParti
     qpart_minmax_kernel<K><<<g, 256, 0, st>>>(Q, q, mm);
     const unsigned gt =
         (unsigned)std::min<uint64_t>((q + part_tile<K>() - 1) / part_tile<K>(), (uint64_t)query_sm_count() * 8);
-    auto padded = [](uint32_t m) { return (m + kPartScanChunk - 1) / kPartScanChunk * kPartScanChunk; };
     const K *src_v = Q;
     const uint32_t *src_i = nullptr;
     uint32_t nseg = 1;
     TL_CUDA_TRY(cudaMemsetAsync(cnt[0], 0, (size_t)padded(kPartBins) * 4, st));
-    qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(0, 0, src_v, src_i, q, mm, ends[1], 1, cnt[0], nullptr, nullptr,
-                                                      nullptr);
-    for (uint32_t pass = 0; pass < kPartPasses; ++pass) {
+    qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(0, bits, 0, src_v, src_i, q, mm, ends[1], 1, cnt[0], nullptr,
+                                                      nullptr, nullptr);
+    for (uint32_t pass = 0; pass < passes; ++pass) {
         const uint32_t m = nseg * kPartBins;  // this pass's buckets
         const uint32_t *seg = ends[(pass + 1) & 1];
         uint32_t *next_ends = ends[pass & 1];
@@ -825,14 +852,14 @@ static int partition_queries(const K *Q, uint64_t q, cudaStream_t st, QueryParti
         const uint32_t chunks = padded(m) / kPartScanChunk;
         qpart_scan_kernel<<<chunks, 1024, 0, st>>>(count, next_ends, total);
         if (chunks > 1) qpart_scan_add_kernel<<<chunks - 1, 1024, 0, st>>>(count, next_ends, total);
-        if (pass + 1 < kPartPasses) {
+        if (pass + 1 < passes) {
             next = cnt[(pass + 1) & 1];
             TL_CUDA_TRY(cudaMemsetAsync(next, 0, (size_t)padded(m * kPartBins) * 4, st));
         }
         K *dv = v[pass & 1];
         uint32_t *di = ix[pass & 1];
-        qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(1, pass, src_v, src_i, q, mm, seg, nseg, count, dv, di,
-                                                          next);
+        qpart_pass_kernel<K><<<gt, kPartThreads, 0, st>>>(1, bits, pass, src_v, src_i, q, mm, seg, nseg, count, dv,
+                                                          di, next);
         src_v = dv;
         src_i = di;
         nseg = m;
@@ -872,19 +899,21 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
     const K *Q = static_cast<const K *>(a.queries);
     uint64_t P = std::min<uint64_t>(a.n, kPinBytes / sizeof(K));
     unsigned grid = 1;
-    // BST and vEB descents over a layout several times L2 search a batch
-    // grouped by value.  Measured on B200, 2^27 queries, as given against
-    // grouped (partition included): BST 2^30 - 1 u64 49.3 / 22.1 ms, 2^26 - 1
-    // u64 29.7 / 15.5 ms; mvEB 2^30 - 1 u32 39.8 / 29.1 ms, 3e8 u32 36.3 /
-    // 27.3 ms, 2^26 - 1 u32 21.0 / 21.8 ms (a 256 MB tree gains nothing).
+    // BST and vEB descents search a batch of 2^21 queries or more grouped by
+    // value, over a vEB layout of 4 MB or more and a BST of 64 MB or more.
+    // Measured on B200, as given against grouped (grouping included): mvEB
+    // 2^30 - 1 u32, 2^27 queries 39.8 / 13.5 ms; mvEB 2^20 - 1 u32, 2^22
+    // queries 0.49 / 0.32 ms, 2^20 queries 0.14 / 0.14; BST 2^23 - 1 u64 (64
+    // MB), 2^22 queries 0.39 / 0.31 ms, 2^20 queries 0.11 / 0.13; BST 2^22 - 1
+    // u64 (32 MB) 0.30 / 0.29 at 2^22 and 9.2 / 11.4 ms at 2^27 queries.
     // B-tree nodes gain little even sorted (9.45 against 8.28 ms) and keep the
     // batch's order.  Measurement hooks: variant 19 never groups, 20 always.
     QueryPartition part;
     const uint32_t *perm = nullptr;
     const uint64_t tree_bytes = a.n * sizeof(K);
-    const bool large = a.layout == Q_BST ? tree_bytes >= (256ull << 20) : tree_bytes >= (1ull << 30);
+    const bool large = a.layout == Q_BST ? tree_bytes >= (64ull << 20) : tree_bytes >= (4ull << 20);
     if ((a.layout == Q_BST || a.layout == Q_VEB || a.layout == Q_VEB_NP) && g_query_variant != 19 &&
-        a.q < (1ull << 32) && (g_query_variant == 20 || (a.q >= (1ull << 20) && large))) {
+        a.q < (1ull << 32) && (g_query_variant == 20 || (a.q >= (1ull << 21) && large))) {
         const int rc = partition_queries<K>(Q, a.q, st, part);
         if (rc == TL_SUCCESS) {
             Q = static_cast<const K *>(part.qs);
@@ -1031,8 +1060,10 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
         // lock-step (2^27 queries over 2^30 - 1 u32 keys: 40.5 ms against 55.5
         // and 55.6; over 3e8 keys 36.6 against 49.0 and 49.3)
         const int qk = g_query_variant == 3 ? 2 : g_query_variant == 4 ? 4 : 1;
-        const size_t budget = qk == 1 ? 48 * 1024 : qk == 2 ? 72 * 1024 : 110 * 1024;
-        const size_t pos_bytes = (size_t)dmax * qk * kVebThreads * (narrow ? 4 : 8);
+        const bool grouped = perm != nullptr && qk == 1;
+        const int threads = grouped ? kVebGroupThreads : kVebThreads;
+        const size_t budget = grouped ? kVebGroupBudget : qk == 1 ? 48 * 1024 : qk == 2 ? 72 * 1024 : 110 * 1024;
+        const size_t pos_bytes = (size_t)dmax * qk * threads * (narrow ? 4 : 8);
         const size_t pin_budget = pos_bytes + kVebMinPin <= budget ? budget - pos_bytes : kVebMinPin;
         P = std::min<uint64_t>(a.n, pin_budget / sizeof(K));
         const size_t smem = (pos_bytes + 15) / 16 * 16 + P * sizeof(K);
@@ -1040,22 +1071,25 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
         auto launch = [&](auto kern, int qpt) -> int {
             TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int per_sm = 0;
-            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kVebThreads, smem));
+            TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
             uint64_t g = (uint64_t)std::max(per_sm, 1) * query_sm_count();
-            uint64_t need = (a.q + (uint64_t)qpt * kVebThreads - 1) / ((uint64_t)qpt * kVebThreads);
+            uint64_t need = (a.q + (uint64_t)qpt * threads - 1) / ((uint64_t)qpt * threads);
             unsigned gr = (unsigned)std::max<uint64_t>(1, std::min(g, need));
-            kern<<<gr, kVebThreads, smem, st>>>(A, a.n, P, dmax, a.tables, np ? a.idx : nullptr,
+            kern<<<gr, threads, smem, st>>>(A, a.n, P, dmax, a.tables, np ? a.idx : nullptr,
                                                 np ? a.table_idx : nullptr, np ? a.num_tables : 1u, Q, a.q, perm,
                                                 a.answers);
             return TL_SUCCESS;
         };
         int rc;
-        if (qk == 1)
-            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 1>, 1) : launch(veb_query_kernel<K, uint64_t, 1>, 1);
+        constexpr int T1 = kVebThreads, TG = kVebGroupThreads;
+        if (grouped)
+            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 1, TG>, 1) : launch(veb_query_kernel<K, uint64_t, 1, TG>, 1);
+        else if (qk == 1)
+            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 1, T1>, 1) : launch(veb_query_kernel<K, uint64_t, 1, T1>, 1);
         else if (qk == 2)
-            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 2>, 2) : launch(veb_query_kernel<K, uint64_t, 2>, 2);
+            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 2, T1>, 2) : launch(veb_query_kernel<K, uint64_t, 2, T1>, 2);
         else
-            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 4>, 4) : launch(veb_query_kernel<K, uint64_t, 4>, 4);
+            rc = narrow ? launch(veb_query_kernel<K, uint32_t, 4, T1>, 4) : launch(veb_query_kernel<K, uint64_t, 4, T1>, 4);
         if (rc) return rc;
     }
     TL_CUDA_TRY(cudaGetLastError());
