@@ -298,6 +298,12 @@ def run_reference(args, rank):
     }))
 
 
+# segments of the learned query's rank model: measured on B200 (2^30 skewed
+# keys, 2^28 queries) 2^16: 1.28x the plain query, 2^18: 1.44x, 2^20: 1.55x,
+# 2^21: 1.57x, 2^22: 1.57x
+LEARNED_LEAVES = 1 << 21
+
+
 def learned_section(args, dev):
     """Learned-start vs plain B-tree queries on skewed keys: n = 2^30 unique
     uint64 keys (lognormal + clusters, seed 8), b = 16, q = 2^28 queries (seed 9,
@@ -316,10 +322,15 @@ def learned_section(args, dev):
     gen_s = time.time() - t0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    model, leaves = LL.train(keys, num_leaves=65536, steps=args.learned_steps, batch=65536, lr=3e-3, seed=1)
+    model, leaves = LL.train(keys, num_leaves=LEARNED_LEAVES, steps=args.learned_steps, batch=65536, lr=3e-3,
+                             seed=1)
     ev1.record()
     torch.cuda.synchronize()
     train_ms = ev0.elapsed_time(ev1)
+    # the same method without the trained root (segments indexed by the
+    # normalised key directly), for the ablation line
+    model0, leaves0 = LL.train(keys, num_leaves=LEARNED_LEAVES, steps=args.learned_steps, batch=65536, lr=3e-3,
+                               seed=1, train_root=False)
     Q = data.zipf_queries_torch(keys, q, 9)
     sorted_keys = keys.clone() if args.parity else None
     T.permute("btree", keys, b)  # keys now hold the layout
@@ -340,6 +351,10 @@ def learned_section(args, dev):
         l_ms.append(LL.query(tree, model, leaves, Q, learned, b, timed=True))
     LL.query(tree, model, leaves, Q, learned, b, stats=stats)
     exact = bool(torch.equal(plain, learned))
+    LL.query(tree, model0, leaves0, Q, learned, b)
+    l0_ms = statistics.median([LL.query(tree, model0, leaves0, Q, learned, b, timed=True) for _ in range(3)])
+    exact0 = bool(torch.equal(plain, learned))
+    del leaves0
     if par is not None:
         par["answers"] = parity_module().check_answers("btree", b, host, Q, plain, 1 << 20, 9)
         del host
@@ -358,8 +373,12 @@ def learned_section(args, dev):
            "fallback_frac": round(int(stats[0].item()) / q, 4),
            "mean_start_depth": round(int(stats[1].item()) / q, 3),
            "train_ms": round(train_ms, 1), "train_loss": model.train_loss, "keygen_s": round(gen_s, 1),
-           "leaves_used": int(used.sum()), "window_median": int(np.median(win)),
-           "window_p99": int(np.percentile(win, 99)), "parity": par}
+           "leaves": LEARNED_LEAVES, "leaves_used": int(used.sum()), "window_median": int(np.median(win)),
+           "window_p99": int(np.percentile(win, 99)),
+           "leaf_only": {"learned_ms": round(l0_ms, 3), "speedup": round(pm / l0_ms, 3), "exact": exact0,
+                         "note": "the same two-stage method with an untrained root (segments indexed by the "
+                                 "normalised key), same keys and queries"},
+           "parity": par}
     del keys, tree, Q, plain, learned, leaves
     torch.cuda.empty_cache()
     return out

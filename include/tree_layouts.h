@@ -309,7 +309,9 @@ typedef struct tl_rank_leaf {
     float slope;       /* ranks per key unit */
     uint32_t eps_lo;   /* largest (prediction - rank) over the segment's keys */
     uint32_t eps_hi;   /* largest (rank - prediction) over the segment's keys */
-    uint32_t empty;    /* 1: no key maps to this segment */
+    uint32_t empty;    /* 1: no key maps to this segment; base and eps_hi
+                          then span the ranks between the nearest segments
+                          below and above that hold keys (slope 0) */
 } tl_rank_leaf;
 
 typedef struct tl_rank_train_config {

@@ -480,6 +480,65 @@ __global__ void leaf_fit_kernel(uint32_t L, const unsigned long long *kmin, cons
     }
 }
 
+// An empty segment's window: the ranks from the largest rank of the nearest
+// segment below that holds keys to the smallest of the nearest one above
+// (where the root is non-decreasing, a query mapped to the empty segment lies
+// between those two keys), as base = the lower, slope 0, eps_hi = the span.
+// One block of 1024 threads, a contiguous run of segments each; a run's
+// nearest holder below and above comes from the runs' summaries.
+__global__ void __launch_bounds__(1024) leaf_fill_empty_kernel(uint32_t L, uint64_t n,
+                                                               const unsigned long long *__restrict__ rmin,
+                                                               const unsigned long long *__restrict__ rmax,
+                                                               tl_rank_leaf *__restrict__ leaves) {
+    constexpr unsigned long long kNone = ~0ull;
+    __shared__ unsigned long long s_last[1024], s_first[1024];
+    const uint32_t per = (L + 1023) / 1024, l0 = min(L, threadIdx.x * per), l1 = min(L, l0 + per);
+    unsigned long long last = kNone, first = kNone;  // this run's last rmax and first rmin of a holder
+    for (uint32_t l = l0; l < l1; ++l)
+        if (rmin[l] <= rmax[l]) {
+            if (first == kNone) first = rmin[l];
+            last = rmax[l];
+        }
+    s_last[threadIdx.x] = last;
+    s_first[threadIdx.x] = first;
+    __syncthreads();
+    if (threadIdx.x == 0) {  // nearest holder before each run / after each run
+        unsigned long long run = kNone;
+        for (int t = 0; t < 1024; ++t) {
+            const unsigned long long v = s_last[t];
+            s_last[t] = run;
+            if (v != kNone) run = v;
+        }
+        run = kNone;
+        for (int t = 1023; t >= 0; --t) {
+            const unsigned long long v = s_first[t];
+            s_first[t] = run;
+            if (v != kNone) run = v;
+        }
+    }
+    __syncthreads();
+    unsigned long long below = s_last[threadIdx.x];
+    for (uint32_t l = l0; l < l1; ++l) {  // the lower end into base
+        if (rmin[l] <= rmax[l]) below = rmax[l];
+        else leaves[l].base = below;
+    }
+    unsigned long long above = s_first[threadIdx.x];
+    for (uint32_t l = l1; l-- > l0;) {
+        if (rmin[l] <= rmax[l]) {
+            above = rmin[l];
+            continue;
+        }
+        const uint64_t lo0 = leaves[l].base == kNone ? 0 : leaves[l].base;
+        const uint64_t hi0 = above == kNone ? n - 1 : above;
+        const uint64_t lo = min(lo0, hi0), hi = max(lo0, hi0);  // a non-monotone root may swap them
+        leaves[l].base = lo;
+        leaves[l].kmin = 0;
+        leaves[l].slope = 0.f;
+        leaves[l].eps_lo = 0;
+        leaves[l].eps_hi = hi - lo > 0xFFFFFFFEull ? 0xFFFFFFFEu : (uint32_t)(hi - lo);
+    }
+}
+
 // The segment's error bounds: the largest over- and under-prediction over its
 // keys, computed with the inference arithmetic itself.
 __global__ void leaf_eps_kernel(const __grid_constant__ ModelParams p, bool use_net, const uint64_t *__restrict__ keys, uint64_t n,
@@ -614,7 +673,7 @@ __device__ __forceinline__ uint64_t learned_start_at(const LearnedGeom &G, const
     const uint64_t n = g.n;
     flags = 0;
     depth = 0;
-    if (lf.empty || g.h == 0) return 0;
+    if (g.h == 0) return 0;
     const uint64_t pr = leaf_predict(lf, q, n);
     const uint64_t rlo = pr > lf.eps_lo ? pr - lf.eps_lo : 0;
     const uint64_t rhi = pr + lf.eps_hi < n ? pr + lf.eps_hi : n - 1;
@@ -1087,6 +1146,7 @@ int rank_model_train(const uint64_t *keys, uint64_t n, const tl_rank_train_confi
     const uint64_t chunks = (n + kLeafChunk - 1) / kLeafChunk;
     leaf_extent_kernel<<<grid_for(chunks, 256), 256, 0, st>>>(p, use_net, keys, n, kmin, kmax, rmin, rmax);
     leaf_fit_kernel<<<grid_for(L, 256), 256, 0, st>>>(L, kmin, kmax, rmin, rmax, leaves);
+    leaf_fill_empty_kernel<<<1, 1024, 0, st>>>(L, n, rmin, rmax, leaves);
     leaf_eps_kernel<<<grid_for(chunks, 256), 256, 0, st>>>(p, use_net, keys, n, leaves);
     TL_CUDA_TRY(cudaGetLastError());
     cudaFreeAsync(buf, st);
