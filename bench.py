@@ -99,6 +99,14 @@ def query_bytes_model(layout, n, b, kb):
     return kb + 8 + fetch * (len(sizes) - l2_levels), l2_levels, len(sizes)
 
 
+def query_grouped(layout, n, kb, q):
+    """Whether the library searches a batch grouped by value first: BST and vEB
+    batches of 2^21 queries or more over a BST layout of 64 MB or more or a vEB
+    layout of 4 MB or more (the thresholds of csrc/query.cu's launch_query)."""
+    return (layout in ("bst", "mveb", "veb") and (1 << 21) <= q < (1 << 32)
+            and n * kb >= (64 << 20 if layout == "bst" else 4 << 20))
+
+
 def query_kernel_name(layout, b, kb):
     """The kernel the library launches for a query batch over a 32-byte aligned
     layout (torch allocations are)."""
@@ -579,7 +587,7 @@ def layouts_section(args, L, dev, stream, local, peak, peak_kind):
                                      for _ in range(3)])
             qbytes, l2lv, nlv = query_bytes_model(layout, n, b or 16, kb)
             qps = q / (qms * 1e-3)
-            grouped = layout != "btree" and q >= 1 << 21 and n * kb >= (64 << 20 if layout == "bst" else 4 << 20)
+            grouped = query_grouped(layout, n, kb, q)
             out[name]["queries"] = {
                 "q": q, "ms": round(qms, 3), "queries_per_s": round(qps, 1),
                 "frac_of_byte_model": round(qps * qbytes / (peak * 1e9), 4), "bytes_per_query": qbytes,
@@ -739,7 +747,8 @@ def run_ours(args, rank, world, local):
                               "roofline_queries_per_s": round(peak * 1e9 / qbytes, 1),
                               "frac": round(qps * qbytes / (peak * 1e9), 4),
                               "model": "w + 8 + one node fetch per level below the L2-resident depth"},
-                 "hits": hits, "kernel": query_kernel_name(layout, b or 16, kb),
+                 "hits": hits, "kernel": query_kernel_name(layout, b or 16, kb)
+                 + (", batch grouped by value" if query_grouped(layout, n, kb, q) else ""),
                  "binary_search_queries_per_s": round(q / (sms * 1e-3), 1),
                  "binary_search_hits": int((sans != n).sum().item())}
         if host_layout is not None:
