@@ -134,7 +134,12 @@ TL_HD uint64_t veb_pos(uint64_t n, uint64_t s, bool modified) {
         uint32_t d = bit_length(nn), rd, ld;
         veb_split(d, modified, rd, ld);
         uint64_t r = low_mask(rd), l = low_mask(ld);
-        uint64_t nf = (nn - r) / l, inc = nn - r - nf * l;
+        // full bottom trees: 2^rd of a perfect tree (no division; every level
+        // of a perfect layout), else a division, 32-bit when it fits
+        uint64_t nf = nn == low_mask(d)          ? r + 1
+                      : nn <= 0xFFFFFFFFull ? (uint64_t)((uint32_t)(nn - r) / (uint32_t)l)
+                                            : (nn - r) / l;
+        uint64_t inc = nn - r - nf * l;
         uint64_t full = nf << ld;  // nf * (l + 1)
         if (s < full) {
             uint64_t i = s >> ld, t = s & l;
@@ -238,7 +243,12 @@ __host__ inline MvebPlan make_mveb_plan(uint64_t n, uint32_t unit_max_levels, ui
         uint32_t d = bit_length(nn), rd, ld;
         veb_split(d, modified, rd, ld);
         uint64_t r = low_mask(rd), l = low_mask(ld);
-        uint64_t nf = (nn - r) / l, inc = nn - r - nf * l;
+        // full bottom trees: 2^rd of a perfect tree (no division; every level
+        // of a perfect layout), else a division, 32-bit when it fits
+        uint64_t nf = nn == low_mask(d)          ? r + 1
+                      : nn <= 0xFFFFFFFFull ? (uint64_t)((uint32_t)(nn - r) / (uint32_t)l)
+                                            : (nn - r) / l;
+        uint64_t inc = nn - r - nf * l;
         uint64_t full = nf << ld;
         MvebRegion u{};
         u.src = src;
