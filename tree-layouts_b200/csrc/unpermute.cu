@@ -66,6 +66,13 @@ __device__ __forceinline__ void gather_runs_warp(const BtreeStream &S, uint64_t 
 }
 
 // B-tree / BST: sorted tile k gathered from the copy C of the layout.
+// The B-tree gather's tile slot of sorted offset o: one padding key after
+// every 32, so the top-tree keys written at stride 2^(k+1) (the BST's levels)
+// spread over the banks (a stride of 4 to 32 keys: 2 to 4 wavefronts a warp
+// instead of 8 to 32), while the final read of consecutive offsets stays
+// conflict-free.
+__device__ __forceinline__ uint32_t gskew(uint32_t o) { return o + (o >> 5); }
+
 template <typename K>
 __global__ void __launch_bounds__(kGatherThreads, 6)
 btree_gather_kernel(K *__restrict__ A, const K *__restrict__ C, const __grid_constant__ BtreeStream S) {
@@ -84,7 +91,7 @@ btree_gather_kernel(K *__restrict__ A, const K *__restrict__ C, const __grid_con
         const Regime &R = gs.reg;
         if (R.kind == 0) {
             for (uint64_t x = p0 + threadIdx.x; x < p1; x += blockDim.x)
-                if (!btree_is_top(S, x)) sm[x - p0] = C[btree_pos(S.g, S.fd, x)];
+                if (!btree_is_top(S, x)) sm[gskew((uint32_t)(x - p0))] = C[btree_pos(S.g, S.fd, x)];
         } else if (R.kind == 1) {
             const K *src = C + R.dbase;
             const uint32_t d = S.fd32.d, r0 = R.r0, skip = R.skip;
@@ -92,7 +99,7 @@ btree_gather_kernel(K *__restrict__ A, const K *__restrict__ C, const __grid_con
             for (uint32_t o = threadIdx.x; o < cnt; o += blockDim.x) {
                 const uint32_t v = r0 + o;
                 const uint32_t ql = S.fd32.div(v);
-                if (v - ql * d != skip) sm[o] = src[v - ql];
+                if (v - ql * d != skip) sm[gskew(o)] = src[v - ql];
             }
         }
         // the tile's top keys, four items a thread at a time: their loads in
@@ -115,10 +122,10 @@ btree_gather_kernel(K *__restrict__ A, const K *__restrict__ C, const __grid_con
             }
 #pragma unroll
             for (int t = 0; t < 4; ++t)
-                if (g0 + t * blockDim.x < total) sm[off[t]] = v[t];
+                if (g0 + t * blockDim.x < total) sm[gskew(off[t])] = v[t];
         }
         __syncthreads();
-        for (uint32_t o = threadIdx.x; o < cnt; o += blockDim.x) A[p0 + o] = sm[o];
+        for (uint32_t o = threadIdx.x; o < cnt; o += blockDim.x) A[p0 + o] = sm[gskew(o)];
         __syncthreads();  // before the next tile reuses the buffer and the runs
     }
 }
@@ -234,10 +241,11 @@ static int launch_unpermute(const PermuteGeometry &geo, K *A, const K *C, cudaSt
         kern<<<(unsigned)grid, kGatherThreads, smem, st>>>(A, C, geo.mp);
     } else {
         auto kern = btree_gather_kernel<K>;
-        TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGatherThreads, smem));
+        const size_t smem_b = smem + (geo.tile_keys / 32 + 1) * sizeof(K);  // gskew's padding keys
+        TL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
+        TL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGatherThreads, smem_b));
         const uint64_t grid = std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * g_gather_sms, geo.ntiles);
-        kern<<<(unsigned)grid, kGatherThreads, smem, st>>>(A, C, geo.bs);
+        kern<<<(unsigned)grid, kGatherThreads, smem_b, st>>>(A, C, geo.bs);
     }
     TL_CUDA_TRY(cudaGetLastError());
     return TL_SUCCESS;
