@@ -48,6 +48,33 @@ def test_training_fits_the_rank_function():
     assert bool((err <= eps.to(torch.int64) & 0xFFFFFFFF).all())
 
 
+def test_empty_segments_take_neighbour_windows():
+    """Segments that no key maps to get the rank window between their nearest
+    key-holding neighbours (slope 0, eps_lo 0, inside [0, n)), so queries that
+    land in them start below the root: with the monotone leaf-only map over
+    2^20 segments for 2^22 keys (most segments empty) the answers equal the
+    plain query's and under 2 % of the queries search from the root."""
+    import torch
+    n, b = 1 << 22, 16
+    keys = _keys(n, seed=8)
+    tree = keys.clone()
+    T.permute("btree", tree, b)
+    model, leaves = LL.train(keys, num_leaves=1 << 20, steps=200, batch=65536, train_root=False)
+    lv = LL.leaves_numpy(leaves)
+    emp = lv["empty"] == 1
+    assert emp.sum() > (1 << 19)
+    assert (lv["slope"][emp] == 0).all() and (lv["eps_lo"][emp] == 0).all()
+    assert (lv["base"][emp].astype(np.uint64) + lv["eps_hi"][emp].astype(np.uint64) <= n - 1).all()
+    Q = data.zipf_queries_torch(keys, 1 << 22, 9)
+    plain = torch.empty(Q.numel(), dtype=torch.int64, device="cuda")
+    learned = torch.empty_like(plain)
+    T.query("btree", tree, Q, plain, b)
+    stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+    LL.query(tree, model, leaves, Q, learned, b, stats=stats)
+    assert torch.equal(plain, learned)
+    assert int(stats[0].item()) / Q.numel() < 0.02, int(stats[0].item()) / Q.numel()
+
+
 @pytest.mark.parametrize("n,b", [(1 << 22, 16), (3_000_017, 16), (2_000_000, 8), (1_048_575, 4)])
 def test_learned_answers_equal_plain_answers(n, b):
     import torch

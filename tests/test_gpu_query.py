@@ -169,6 +169,35 @@ def test_veb_query_kernel_forms(variant, layout):
         L.tl_debug_set_query_variant(0)
 
 
+@pytest.mark.parametrize("layout,n,kb,q", [("mveb", 2**24 - 1, 4, 2**23), ("bst", 2**23 - 1, 8, 2**23),
+                                           ("mveb", 2**24 - 1, 4, 2**27)])
+def test_grouped_queries_at_16_and_20_bucket_bits(layout, n, kb, q):
+    """Batches large enough for 16 bucket bits (2^23 queries: four passes) and
+    for 20 (2^27: five passes), grouped by default, equal the same batches
+    searched as given (variant 19)."""
+    import ctypes as C
+
+    import torch
+    L = T.lib()
+    L.tl_debug_set_query_variant.argtypes = [C.c_int]
+    keys = data.sorted_keys_torch(n, 1, 3 if kb == 4 else 16, n % 1000 + 3, kb)
+    tree = keys.clone()
+    T.permute(layout, tree, 16)
+    tabs = T.VebTablesDevice(n, "cuda", standard=layout == "veb") if layout != "bst" else None
+    Q = data.queries_torch(keys, q, 0.5, 11)
+    got = torch.empty(q, dtype=torch.int64, device="cuda")
+    exp = torch.empty_like(got)
+    T.query(layout, tree, Q, got, 16, tables=tabs)  # default: grouped at these sizes
+    try:
+        L.tl_debug_set_query_variant(19)
+        T.query(layout, tree, Q, exp, 16, tables=tabs)
+    finally:
+        L.tl_debug_set_query_variant(0)
+    assert torch.equal(got, exp), (layout, n, q)
+    hit = got != n
+    assert torch.equal(tree[got[hit]], Q[hit])
+
+
 @pytest.mark.parametrize("layout,n,kb", [("mveb", 2**24 - 1, 4), ("mveb", 20_000_003, 4), ("veb", 2**22 - 1, 8),
                                          ("bst", 2**23 - 1, 8), ("bst", 9_000_001, 4)])
 def test_partitioned_queries_match_unpartitioned(layout, n, kb):
