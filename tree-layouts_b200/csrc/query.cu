@@ -18,6 +18,11 @@ namespace tl {
 
 constexpr int kQueryThreads = 256;
 constexpr uint32_t kPinBytes = 48 * 1024;
+// A grouped batch over a BST of 256 MB or more pins fewer top levels, leaving
+// room for 8 blocks an SM: measured on B200, 2^27 grouped queries, 2^30 - 1 u64
+// keys 13.25 -> 12.14 ms, 2^27 - 1 u32 10.23 -> 9.79 ms (8 KB: the same); over
+// a 128 MB tree 11.0 -> 11.6 ms, so not there
+constexpr uint32_t kBstGroupPinBytes = 16 * 1024;
 
 template <typename K>
 __device__ __forceinline__ void pin_prefix(const K *__restrict__ A, uint64_t P, K *sm) {
@@ -933,7 +938,9 @@ static int launch_query(const QueryArgs &a, cudaStream_t st) {
         if (rc) return rc;
         kern<<<grid, kQueryThreads, smem, st>>>(A, a.n, L, Q, a.q, a.answers);
     } else if (a.layout == Q_BST) {
-        // whole top levels: 2^T - 1 keys
+        // whole top levels: 2^T - 1 keys (a grouped batch over a large tree:
+        // at most kBstGroupPinBytes of them, leaving room for more blocks)
+        if (perm && tree_bytes >= (256ull << 20)) P = std::min<uint64_t>(P, kBstGroupPinBytes / sizeof(K));
         uint64_t top = 1;
         while (top * 2 + 1 <= P) top = top * 2 + 1;
         P = std::min<uint64_t>(top, a.n);
